@@ -1,0 +1,387 @@
+#!/usr/bin/env python
+"""Benchmark: weighted-minhash throughput (nnz*samples evaluations/s) on B200.
+
+Default workload ("large"): one 2,000,000 x 1,000,000 fp32 CSR matrix, row
+nnz ~ Poisson(1400) (~2.8e9 nnz), Zipf(1.1) columns, lognormal values, 128
+samples, generator seed 2.  Inputs (22.4 GB of CSR) and the parameter table
+(1.5 GB) are far larger than the 126 MB L2, so no L2 flush is needed between
+steps.
+
+  value  device throughput: the CSR is resident in HBM, one step is one
+         mhcuda_calc_device call (plan + hash + finalize kernels), timed with
+         CUDA events on the launch stream.
+  e2e    the same metric through the drop-in C ABI call mhcuda_calc with
+         pinned host buffers: every step copies the CSR host->device and the
+         hashes device->host inside the timed region.
+  roofline  the hash kernel alone, timed with events the library records
+         around each launch on its stream; algorithmic bytes per launch
+         B = 12*N*S + 8*N + 4*(R+1) + 8*R*S over the measured HBM copy
+         bandwidth.
+  cpu_baseline  the C oracle (oracle/wmh_oracle.c, OpenMP on all host cores)
+         on a bounded sample of the same rows, which is also checked bit for
+         bit against the GPU's output for those rows.
+
+--impl reference runs the reference arm: the reference has no CPU
+implementation of the hash (kernel.cu is CUDA only), so it times the C oracle
+port of the reference kernel on all host cores over a bounded sample of the
+same workload per step.
+
+Multi-GPU: the path has no exchange step; N ranks run N independent replicas
+(weak scaling, one process per GPU, no data-path collective).  Timing is the
+max over ranks of the per-rank device time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "WMH nnz*samples/s (plain calc, 1 B200, bit-exact)"
+UNIT = "nnz*samples/s"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def dist_setup():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Clocks:
+    """Samples nvidia-smi clocks / throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 9 and f[1].replace(".", "").isdigit():
+                    rows.append(f)
+        except OSError:
+            pass
+        finally:
+            if self.path and os.path.exists(self.path):
+                os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v == "Active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(float(r[2]) for r in rows),
+                "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit()),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_oracle_sample(w, params_host, target_s=12.0, check=None, nthreads=0, max_rows=20000):
+    """Times the C oracle on the first rows of the workload, growing the
+    sample until it takes ~target_s.  Returns (evals/s, rows, nnz, seconds,
+    bit_exact or None)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from minhashcuda_b200 import synth
+    co = O.COracle(*params_host)
+    rows = 64
+    while True:
+        ip, cols, wts = synth.host_csr(w, 0, rows)
+        t0 = time.perf_counter()
+        out = co.hash(wts, cols, ip, threads=nthreads)
+        dt = time.perf_counter() - t0
+        if dt >= target_s / 4 or rows >= max_rows:
+            break
+        rows = min(max_rows, int(rows * max(2.0, min(8.0, (target_s / 4) / max(dt, 1e-3)))))
+    nnz = int(ip[-1])
+    exact = None
+    if check is not None:
+        exact = check(rows, ip, cols, wts, co)
+    return nnz * w.samples / dt, rows, nnz, dt, exact
+
+
+def run_reference_arm(args, rank):
+    """--impl reference: the C oracle port on all host cores, K timed steps of a
+    bounded sample of the workload."""
+    if rank != 0:
+        return
+    import torch
+    from minhashcuda_b200 import synth
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    w = synth.WORKLOADS[args.workload]
+    torch.cuda.set_device(0)
+    g = np.random.default_rng(w.seed)
+    # The oracle only reads the parameter table; a seeded Gamma/uniform table
+    # has the generator's distributions (its values do not change the work).
+    rs = g.gamma(2.0, 1.0, (w.samples, w.dim)).astype(np.float32)
+    lc = np.log(g.gamma(2.0, 1.0, (w.samples, w.dim))).astype(np.float32)
+    bt = g.uniform(0, 1, (w.samples, w.dim)).astype(np.float32)
+    co = O.COracle(rs, lc, bt)
+    del rs, lc, bt
+    rows = args.cpu_rows
+    ip, cols, wts = synth.host_csr(w, 0, rows)
+    nnz = int(ip[-1])
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        co.hash(wts, cols, ip, threads=threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        co.hash(wts, cols, ip, threads=threads)
+        times.append(time.perf_counter() - t0)
+    t = sum(times) / len(times)
+    value = nnz * w.samples / t
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": workload_config(w, args),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"first {rows} rows ({nnz} nnz) of the workload per step; the "
+                                   "reference has no CPU hash path, so this is the C port of "
+                                   "kernel.cu:95-110 (oracle/wmh_oracle.c)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "rows_per_s": rows / t,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(w, args):
+    return {"workload": f"{w.name}: {w.rows} rows x {w.dim} dims, samples {w.samples}, "
+                        f"row nnz {['Poisson', 'lognormal', 'log-uniform', 'Zipf'][w.nnz_kind]}"
+                        f"({w.nnz_p1:g}{', %g' % w.nnz_p2 if w.nnz_p2 else ''}), {w.cols} columns, "
+                        "lognormal(0,1) values",
+            "rows": w.rows, "dim": w.dim, "samples": w.samples, "seed": w.seed,
+            "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas{args.gpus}"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="large", choices=["large"])
+    ap.add_argument("--rows", type=int, default=0, help="override the row count (smaller runs)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-rows", type=int, default=3000)
+    args = ap.parse_args()
+
+    rank, world, local = dist_setup()
+    if args.impl == "reference":
+        return run_reference_arm(args, rank)
+
+    import torch
+    import minhashcuda_b200 as mb
+    from minhashcuda_b200 import synth
+
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    w = synth.WORKLOADS[args.workload]
+    if args.rows:
+        w = synth.Workload(**{**w.__dict__, "rows": args.rows})
+    lib = mb.capi()
+    dev_mask = 1 << local
+
+    # ---- generator (cuRAND, seed) and device-resident workload -------------
+    status = ctypes.c_int(-1)
+    t0 = time.perf_counter()
+    gen = lib.mhcuda_init(w.dim, w.samples, w.seed, 0, dev_mask, 0, ctypes.byref(status))
+    assert gen, f"mhcuda_init failed: {status.value}"
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        indptr, cols, weights, nnz = synth.device_csr(w, 0, w.rows, stream=stream)
+    torch.cuda.synchronize()
+    log(f"[rank {rank}] workload {w.name}: rows={w.rows} nnz={nnz} "
+        f"generated in {time.perf_counter() - t0:.1f}s")
+    R, S = w.rows, w.samples
+    out = torch.empty((R, S, 2), dtype=torch.int32, device="cuda")
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+
+    def step():
+        rc = lib.mhcuda_calc_device(gen, weights.data_ptr(), cols.data_ptr(), indptr.data_ptr(),
+                                    R, nnz, out.data_ptr(), sptr)
+        assert rc == 0, rc
+
+    def barrier():
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+
+    def max_over_ranks(x):
+        if not pg:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- value: device-resident throughput ---------------------------------
+    for _ in range(args.warmup):
+        step()
+    assert lib.mhcuda_device_status(gen) == 0, "device reported invalid CSR"
+    barrier()
+    lib.mhcuda_profile(gen, 1)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms_total = ev0.elapsed_time(ev1)
+    hash_ms = ctypes.c_double(0)
+    launches = ctypes.c_uint64(0)
+    assert lib.mhcuda_profile_read(gen, ctypes.byref(hash_ms), ctypes.byref(launches)) == 0
+    lib.mhcuda_profile(gen, 0)
+    clocks = clk.summary()
+    barrier()
+    ms_step = max_over_ranks(ms_total / args.steps)
+    evals = nnz * S
+    value = evals * world / (ms_step / 1e3)
+
+    hash_ms_launch = hash_ms.value / max(1, launches.value)
+    alg_bytes = 12 * nnz * S + 8 * nnz + 4 * (R + 1) + 8 * R * S
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / (hash_ms_launch / 1e3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": None, "kernel": "hash_kernel",
+                "kernel_ms": hash_ms_launch, "algorithmic_bytes": alg_bytes,
+                "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)"}
+
+    # ---- parity spot check + CPU baseline (rank 0) -----------------------------
+    cpu = None
+    parity = None
+    if rank == 0 and not args.no_cpu:
+        params = [np.empty((S, w.dim), np.float32) for _ in range(3)]
+        assert lib.mhcuda_retrieve_random_vars(gen, *[p.ctypes.data for p in params]) == 0
+        gpu_out = out.cpu().numpy().view(np.uint32)
+
+        def check(rows, ip, cl, wt, co):
+            lnw = np.empty_like(wt)
+            assert lib.mhcuda_debug_device_logf(dev_mask, wt.ctypes.data, lnw.ctypes.data,
+                                                wt.size) == 0
+            want = co.hash(wt, cl, ip, lnw=lnw)
+            return bool(np.array_equal(want, gpu_out[:rows]))
+
+        v, rows_s, nnz_s, dt, exact = cpu_oracle_sample(w, params, check=check)
+        cores = os.cpu_count()
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"first {rows_s} rows ({nnz_s} nnz x {S} samples) of the workload, "
+                         f"{dt:.2f}s on {cores} threads (C oracle, OpenMP)"}
+        parity = {"rows_checked": rows_s, "bit_exact": exact}
+        del params, gpu_out
+
+    # ---- e2e through the drop-in C ABI with pinned host buffers ----------------
+    e2e = None
+    if not args.no_e2e:
+        h_w = torch.empty(nnz, dtype=torch.float32, pin_memory=True)
+        h_c = torch.empty(nnz, dtype=torch.int32, pin_memory=True)
+        h_i = torch.empty(R + 1, dtype=torch.int32, pin_memory=True)
+        h_o = torch.empty((R, S, 2), dtype=torch.int32, pin_memory=True)
+        h_w.copy_(weights[:nnz])
+        h_c.copy_(cols[:nnz])
+        h_i.copy_(indptr)
+        del weights, cols  # the e2e path stages its own device copy
+        torch.cuda.empty_cache()
+
+        def e2e_step():
+            rc = lib.mhcuda_calc(gen, h_w.data_ptr(), h_c.data_ptr(), h_i.data_ptr(), R,
+                                 h_o.data_ptr())
+            assert rc == 0, rc
+
+        for _ in range(min(args.warmup, 3)):
+            e2e_step()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record()
+        for _ in range(args.steps):
+            e2e_step()
+        e1.record()
+        torch.cuda.synchronize()
+        wall = (time.perf_counter() - t0) / args.steps
+        e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+        same = bool(torch.equal(h_o.cuda(), out))
+        e2e = {"value": evals * world / (e2e_ms / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": 8 * nnz + 4 * (R + 1), "d2h_bytes_per_step": 8 * R * S,
+               "ms_per_step": e2e_ms, "wall_ms_per_step": wall * 1e3,
+               "matches_device_path": same}
+    lib.mhcuda_fini(gen)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded, generated on the device)",
+            "config": workload_config(w, args), "rows_per_s": R * world / (ms_step / 1e3),
+            "nnz": nnz, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "parity": parity, "clocks": clocks,
+            "gpu_launches": 3 * args.steps,
+        }
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,75 @@
+/*
+ * minhashcuda_b200.h -- entry points this engine adds beside the drop-in ABI
+ * of minhashcuda.h.  All are extern "C", take plain pointers and sizes, and
+ * return the same MHCUDAResult codes.  Device pointers must belong to the
+ * generator's device; a `stream` argument is a cudaStream_t passed as void*
+ * (NULL selects the generator's own stream).
+ */
+#ifndef MHCUDA_MINHASHCUDA_B200_H
+#define MHCUDA_MINHASHCUDA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "minhashcuda.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Device-resident counterpart of mhcuda_calc (minhashcuda.h:115-118): the
+ * CSR (d_weights/d_cols with `nnz` entries, d_rows with length+1 offsets
+ * whose first value is the offset of d_weights[0]) and d_output
+ * (length*samples*2 uint32) already live in device memory.  The work is
+ * enqueued on `stream` and the call returns without waiting; the generator's
+ * scratch is reused by the next call on it, so calls on one generator must
+ * be ordered on one stream.  Invalid CSR content (a column >= dim,
+ * decreasing offsets) is detected on the device and reported by the next
+ * mhcuda_device_status() call. */
+enum MHCUDAResult mhcuda_calc_device(
+    const MinhashCudaGenerator *gen, const float *d_weights,
+    const uint32_t *d_cols, const uint32_t *d_rows, uint32_t length,
+    uint32_t nnz, uint32_t *d_output, void *stream);
+
+/* Waits for the generator's device work and returns mhcudaInvalidArguments
+ * if a preceding mhcuda_calc_device saw invalid CSR content (and clears the
+ * flag), mhcudaRuntimeError on a CUDA error, else mhcudaSuccess.
+ * No counterpart in the reference (its kernel launch is unchecked,
+ * kernel.cu:166-170). */
+enum MHCUDAResult mhcuda_device_status(const MinhashCudaGenerator *gen);
+
+/* Hashes `count` independent CSR matrices (host buffers, as in mhcuda_calc)
+ * against one generator in one device pass: the matrices are staged
+ * back to back, one persistent launch walks a (matrix, row-chunk) work list
+ * and each matrix's hashes land in outputs[i] (lengths[i]*samples*2 uint32).
+ * Equivalent to `count` mhcuda_calc calls (minhashcuda.h:115-118), bit for
+ * bit.  A matrix with lengths[i] == 0 is skipped. */
+enum MHCUDAResult mhcuda_calc_batch(
+    const MinhashCudaGenerator *gen, uint32_t count,
+    const float *const *weights, const uint32_t *const *cols,
+    const uint32_t *const *rows, const uint32_t *lengths,
+    uint32_t *const *outputs);
+
+/* Test hook: evaluates the device logf (the one the hash kernel applies to
+ * every weight) on n host floats, on the device selected like mhcuda_init's
+ * `devices` mask.  No counterpart in the reference. */
+enum MHCUDAResult mhcuda_debug_device_logf(
+    uint32_t devices, const float *in, float *out, uint64_t n);
+
+/* Starts (enable != 0) or stops timing every hash-kernel launch of the
+ * generator with CUDA events recorded on the launch stream, and clears the
+ * accumulated figures.  No counterpart in the reference (its build
+ * defines PROFILE, CMakeLists.txt:9-11, but no source reads it). */
+enum MHCUDAResult mhcuda_profile(const MinhashCudaGenerator *gen, int enable);
+
+/* Waits for the timed launches and returns their summed device time in ms
+ * and their count since the last mhcuda_profile/mhcuda_profile_read call,
+ * then clears them.  No counterpart in the reference. */
+enum MHCUDAResult mhcuda_profile_read(const MinhashCudaGenerator *gen, double *hash_ms,
+                                      uint64_t *launches);
+
+#ifdef __cplusplus
+}  /* extern "C" */
+#endif
+
+#endif  /* MHCUDA_MINHASHCUDA_B200_H */

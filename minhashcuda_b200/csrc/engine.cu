@@ -1,0 +1,666 @@
+// Host engine: generator lifetime, parameter init/IO, the calc drivers and
+// the extern "C" entry points of include/minhashcuda.h and
+// include/minhashcuda_b200.h.
+//
+// Replaces the reference's host runtime (minhashcuda.cc of
+// src-d/minhashcuda) for one device:
+//  - device choice: the lowest present device in the mask, no compute
+//    capability filter (minhashcuda.cc:43-110 keeps several and drops CCs it
+//    was not built for);
+//  - no host binpacking (minhashcuda.cc:457-528): the hash launch cuts work
+//    by nnz on the device (hash_kernels.cu);
+//  - grow-only device workspace as in minhashcuda.cc:385-455, but sizes and
+//    offsets are 64-bit and every launch is checked.
+#include <algorithm>
+#include <cinttypes>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include <cuda_runtime.h>
+#include <curand.h>
+
+#include "../../include/minhashcuda.h"
+#include "../../include/minhashcuda_b200.h"
+#include "wmh_internal.h"
+
+using mhb::HashArgs;
+using mhb::HashPlan;
+
+namespace {
+
+#define MHB_INFO(gen, ...) \
+  do { if ((gen)->verbosity > 0) { printf(__VA_ARGS__); fflush(stdout); } } while (0)
+#define MHB_DEBUG(gen, ...) \
+  do { if ((gen)->verbosity > 1) { printf(__VA_ARGS__); fflush(stdout); } } while (0)
+
+// Returns `code` from the enclosing function when `call` fails.
+#define MHB_CHECK(gen, call, code)                                                  \
+  do {                                                                              \
+    cudaError_t err__ = (call);                                                     \
+    if (err__ != cudaSuccess) {                                                     \
+      MHB_INFO(gen, "%s:%d -> %s\n", __FILE__, __LINE__, cudaGetErrorString(err__)); \
+      return code;                                                                  \
+    }                                                                               \
+  } while (0)
+
+struct DevBuf {
+  void *ptr = nullptr;
+  size_t cap = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    cap = 0;
+  }
+  // Grow-only; contents are not preserved across growth.
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= cap && ptr) return cudaSuccess;
+    release();
+    const size_t want = std::max<size_t>(bytes, 256);
+    cudaError_t e = cudaMalloc(&ptr, want);
+    if (e != cudaSuccess) {
+      ptr = nullptr;
+      cudaGetLastError();
+      return e;
+    }
+    cap = want;
+    return cudaSuccess;
+  }
+  template <typename T>
+  T *as() const { return static_cast<T *>(ptr); }
+};
+
+struct PinnedBuf {
+  void *ptr = nullptr;
+  size_t cap = 0;
+  PinnedBuf() = default;
+  PinnedBuf(const PinnedBuf &) = delete;
+  PinnedBuf &operator=(const PinnedBuf &) = delete;
+  ~PinnedBuf() { release(); }
+  void release() {
+    if (ptr) cudaFreeHost(ptr);
+    ptr = nullptr;
+    cap = 0;
+  }
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= cap && ptr) return cudaSuccess;
+    release();
+    const size_t want = std::max<size_t>(bytes, 4096);
+    cudaError_t e = cudaHostAlloc(&ptr, want, cudaHostAllocPortable);
+    if (e != cudaSuccess) {
+      ptr = nullptr;
+      cudaGetLastError();
+      return e;
+    }
+    cap = want;
+    return cudaSuccess;
+  }
+  template <typename T>
+  T *as() const { return static_cast<T *>(ptr); }
+};
+
+int env_int(const char *name, int fallback) {
+  const char *v = getenv(name);
+  if (!v || !*v) return fallback;
+  return atoi(v);
+}
+
+}  // namespace
+
+// The generator.  Opaque to callers (minhashcuda.h declares only the tag).
+struct MinhashCudaGenerator_ {
+  uint32_t dim = 0;
+  uint16_t samples = 0;
+  int verbosity = 0;
+  int device = 0;
+  uint32_t s_pad = 0;
+  int sm_count = 0;
+  float *params = nullptr;  // [dim][3][s_pad]
+  cudaStream_t stream = nullptr;
+
+  // Serialises calls on one generator (the reference's generator is not
+  // re-entrant either: minhashcuda.cc:27-34 holds mutable buffers).
+  mutable std::mutex mu;
+  // Grow-only workspace.
+  mutable DevBuf d_weights, d_cols, d_indptr, d_out, d_chunk_row, d_part_ln, d_part_kt, d_status;
+  mutable PinnedBuf h_status;
+  mutable PinnedBuf h_stage;      // batch staging (weights | cols | indptr)
+  // Optional timing of every hash-kernel launch with CUDA events recorded on
+  // the launch stream (mhcuda_profile / mhcuda_profile_read).
+  mutable bool profiling = false;
+  mutable std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
+  mutable size_t prof_used = 0;
+
+  ~MinhashCudaGenerator_() {
+    cudaSetDevice(device);
+    if (stream) cudaStreamSynchronize(stream);
+    d_weights.release(); d_cols.release(); d_indptr.release(); d_out.release();
+    d_chunk_row.release(); d_part_ln.release(); d_part_kt.release(); d_status.release();
+    h_status.release(); h_stage.release();
+    for (auto &e : prof_events) {
+      cudaEventDestroy(e.first);
+      cudaEventDestroy(e.second);
+    }
+    if (params) cudaFree(params);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+using Gen = MinhashCudaGenerator_;
+
+// Lowest device named by the mask that exists; mask 0 means device 0.
+int pick_device(uint32_t devices) {
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) {
+    cudaGetLastError();
+    return -1;
+  }
+  if (devices == 0) return 0;
+  for (int d = 0; d < 32 && d < count; ++d) {
+    if (devices & (1u << d)) return d;
+  }
+  return -1;
+}
+
+// Chooses samples-per-lane, chunk size and grid for one launch.
+HashPlan make_plan(const Gen *gen, uint64_t nnz, uint64_t rows) {
+  HashPlan p{};
+  const uint32_t s_pad = gen->s_pad;
+  int spl = env_int("MHCUDA_B200_SPL", 0);
+  if (spl != 1 && spl != 2 && spl != 4) {
+    // Wide tiles amortise the per-nnz overhead (shuffles, addressing, the
+    // logf share); narrow tiles give small inputs more warps.  Keep lane
+    // utilisation of the last tile >= 3/4.
+    const uint64_t evals = nnz * static_cast<uint64_t>(gen->samples);
+    spl = 4;
+    auto util = [&](int s) {
+      const uint32_t w = 32u * s;
+      const uint32_t tiles = (s_pad + w - 1) / w;
+      return static_cast<double>(s_pad) / (static_cast<double>(tiles) * w);
+    };
+    if (util(4) < 0.75) spl = util(2) >= 0.75 ? 2 : 1;
+    if (evals < (1ull << 26) && spl > 1) spl = 1;  // small inputs: more items
+  }
+  p.spl = static_cast<uint32_t>(spl);
+  const uint32_t tile_w = 32u * p.spl;
+  p.ntiles = (s_pad + tile_w - 1) / tile_w;
+  const int bps = mhb::hash_blocks_per_sm(p.spl);
+  const uint64_t resident_warps =
+      static_cast<uint64_t>(gen->sm_count) * bps * (mhb::kHashBlock / 32);
+  const int waves = std::max(1, env_int("MHCUDA_B200_WAVES", 32));
+  const uint64_t target_items = resident_warps * waves;
+  uint64_t chunk = (nnz * p.ntiles + target_items - 1) / target_items;
+  // Rows shorter than a chunk finish inside it; aim for a few rows per chunk.
+  const uint64_t avg_row = rows ? (nnz + rows - 1) / rows : 1;
+  chunk = std::max<uint64_t>(chunk, std::min<uint64_t>(4 * avg_row, 1024));
+  const int forced = env_int("MHCUDA_B200_CHUNK", 0);
+  if (forced > 0) chunk = static_cast<uint64_t>(forced);
+  chunk = std::max<uint64_t>(64, (chunk + 31) & ~31ull);
+  chunk = std::min<uint64_t>(chunk, 1u << 24);
+  p.chunk = static_cast<uint32_t>(chunk);
+  const uint64_t nchunks = nnz == 0 ? 1 : (nnz + chunk - 1) / chunk;
+  p.nchunks = static_cast<uint32_t>(nchunks);
+  const uint64_t items = nchunks * p.ntiles;
+  const uint64_t want_blocks = (items + (mhb::kHashBlock / 32) - 1) / (mhb::kHashBlock / 32);
+  const uint64_t max_blocks = static_cast<uint64_t>(gen->sm_count) * bps;
+  p.grid = static_cast<uint32_t>(std::max<uint64_t>(1, std::min(want_blocks, max_blocks)));
+  return p;
+}
+
+// Ensures the per-launch workspace and fills the device-side arguments.
+MHCUDAResult prepare_launch(const Gen *gen, uint32_t rows, uint32_t nnz, const HashPlan &plan,
+                            HashArgs *a) {
+  const size_t slots = static_cast<size_t>(plan.nchunks) * 2;
+  MHB_CHECK(gen, gen->d_chunk_row.ensure(static_cast<size_t>(plan.nchunks) * 4),
+            mhcudaMemoryAllocationFailure);
+  MHB_CHECK(gen, gen->d_part_ln.ensure(slots * gen->s_pad * sizeof(float)),
+            mhcudaMemoryAllocationFailure);
+  MHB_CHECK(gen, gen->d_part_kt.ensure(slots * gen->s_pad * sizeof(uint2)),
+            mhcudaMemoryAllocationFailure);
+  MHB_CHECK(gen, gen->d_status.ensure(sizeof(uint32_t)), mhcudaMemoryAllocationFailure);
+  a->params = gen->params;
+  a->dim = gen->dim;
+  a->samples = gen->samples;
+  a->s_pad = gen->s_pad;
+  a->rows = rows;
+  a->nnz = nnz;
+  a->chunk = plan.chunk;
+  a->nchunks = plan.nchunks;
+  a->ntiles = plan.ntiles;
+  a->chunk_row = gen->d_chunk_row.as<uint32_t>();
+  a->part_ln = gen->d_part_ln.as<float>();
+  a->part_kt = gen->d_part_kt.as<uint2>();
+  a->status = gen->d_status.as<uint32_t>();
+  return mhcudaSuccess;
+}
+
+MHCUDAResult enqueue_hash(const Gen *gen, const HashArgs &a, const HashPlan &plan,
+                          cudaStream_t stream) {
+  MHB_CHECK(gen, cudaMemsetAsync(a.status, 0, sizeof(uint32_t), stream), mhcudaRuntimeError);
+  MHB_CHECK(gen, mhb::launch_plan(a, stream), mhcudaRuntimeError);
+  std::pair<cudaEvent_t, cudaEvent_t> *ev = nullptr;
+  if (gen->profiling) {
+    if (gen->prof_used == gen->prof_events.size()) {
+      std::pair<cudaEvent_t, cudaEvent_t> e{nullptr, nullptr};
+      MHB_CHECK(gen, cudaEventCreate(&e.first), mhcudaRuntimeError);
+      MHB_CHECK(gen, cudaEventCreate(&e.second), mhcudaRuntimeError);
+      gen->prof_events.push_back(e);
+    }
+    ev = &gen->prof_events[gen->prof_used++];
+    MHB_CHECK(gen, cudaEventRecord(ev->first, stream), mhcudaRuntimeError);
+  }
+  MHB_CHECK(gen, mhb::launch_hash(a, plan, stream), mhcudaRuntimeError);
+  if (ev) MHB_CHECK(gen, cudaEventRecord(ev->second, stream), mhcudaRuntimeError);
+  if (plan.nchunks > 1) MHB_CHECK(gen, mhb::launch_finalize(a, stream), mhcudaRuntimeError);
+  return mhcudaSuccess;
+}
+
+MHCUDAResult read_status(const Gen *gen, cudaStream_t stream) {
+  MHB_CHECK(gen, gen->h_status.ensure(sizeof(uint32_t)), mhcudaMemoryAllocationFailure);
+  uint32_t *h = gen->h_status.as<uint32_t>();
+  MHB_CHECK(gen, cudaMemcpyAsync(h, gen->d_status.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                 stream),
+            mhcudaMemoryCopyError);
+  MHB_CHECK(gen, cudaStreamSynchronize(stream), mhcudaRuntimeError);
+  if (*h != 0) {
+    MHB_INFO(gen, "invalid CSR input (status 0x%x)\n", *h);
+    return mhcudaInvalidArguments;
+  }
+  return mhcudaSuccess;
+}
+
+MHCUDAResult init_params(Gen *gen, uint32_t seed) {
+  const size_t n = static_cast<size_t>(gen->dim) * gen->samples;
+  DevBuf a, b;
+  MHB_CHECK(gen, a.ensure(n * sizeof(float)), mhcudaMemoryAllocationFailure);
+  MHB_CHECK(gen, b.ensure(n * sizeof(float)), mhcudaMemoryAllocationFailure);
+  curandGenerator_t rng = nullptr;
+  auto fail = [&](MHCUDAResult code) {
+    if (rng) curandDestroyGenerator(rng);
+    return code;
+  };
+  // The same generator type, seed and five draws of n floats as
+  // minhashcuda.cc:181-199, so a seed reproduces the reference's table.
+  if (curandCreateGenerator(&rng, CURAND_RNG_PSEUDO_DEFAULT) != CURAND_STATUS_SUCCESS)
+    return fail(mhcudaRuntimeError);
+  if (curandSetStream(rng, gen->stream) != CURAND_STATUS_SUCCESS ||
+      curandSetPseudoRandomGeneratorSeed(rng, seed) != CURAND_STATUS_SUCCESS)
+    return fail(mhcudaRuntimeError);
+  float *A = a.as<float>(), *B = b.as<float>();
+  const uint32_t D = gen->dim, S = gen->samples, P = gen->s_pad;
+  // rs = -logf(U2 * U1)
+  if (curandGenerateUniform(rng, A, n) != CURAND_STATUS_SUCCESS ||
+      curandGenerateUniform(rng, B, n) != CURAND_STATUS_SUCCESS)
+    return fail(mhcudaRuntimeError);
+  if (mhb::launch_pack_params(A, B, mhb::PairOp::kGamma, 0, D, S, P, gen->params, gen->stream) !=
+      cudaSuccess)
+    return fail(mhcudaRuntimeError);
+  // ln_cs = logf(-logf(U3 * U4))
+  if (curandGenerateUniform(rng, A, n) != CURAND_STATUS_SUCCESS ||
+      curandGenerateUniform(rng, B, n) != CURAND_STATUS_SUCCESS)
+    return fail(mhcudaRuntimeError);
+  if (mhb::launch_pack_params(A, B, mhb::PairOp::kLogGamma, 1, D, S, P, gen->params,
+                              gen->stream) != cudaSuccess)
+    return fail(mhcudaRuntimeError);
+  // betas = U5
+  if (curandGenerateUniform(rng, A, n) != CURAND_STATUS_SUCCESS) return fail(mhcudaRuntimeError);
+  if (mhb::launch_pack_params(A, nullptr, mhb::PairOp::kCopy, 2, D, S, P, gen->params,
+                              gen->stream) != cudaSuccess)
+    return fail(mhcudaRuntimeError);
+  if (cudaStreamSynchronize(gen->stream) != cudaSuccess) return fail(mhcudaRuntimeError);
+  curandDestroyGenerator(rng);
+  return mhcudaSuccess;
+}
+
+}  // namespace
+
+extern "C" {
+
+MinhashCudaGenerator *mhcuda_init(uint32_t dim, uint16_t samples, uint32_t seed, int deferred,
+                                  uint32_t devices, int verbosity, enum MHCUDAResult *status) {
+  auto set = [&](MHCUDAResult r) {
+    if (status) *status = r;
+  };
+  if (dim == 0 || samples == 0) {
+    set(mhcudaInvalidArguments);
+    return nullptr;
+  }
+  const int dev = pick_device(devices);
+  if (dev < 0 || cudaSetDevice(dev) != cudaSuccess) {
+    cudaGetLastError();
+    set(mhcudaNoSuchDevice);
+    return nullptr;
+  }
+  std::unique_ptr<Gen> gen(new Gen());
+  gen->dim = dim;
+  gen->samples = samples;
+  gen->verbosity = verbosity;
+  gen->device = dev;
+  gen->s_pad = mhb::padded_samples(samples);
+  if (cudaDeviceGetAttribute(&gen->sm_count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    set(mhcudaNoSuchDevice);
+    return nullptr;
+  }
+  MHB_DEBUG(gen.get(), "mhcuda_init: dim=%" PRIu32 " samples=%" PRIu16 " seed=%" PRIu32
+            " deferred=%d device=%d\n", dim, samples, seed, deferred, dev);
+  if (cudaStreamCreateWithFlags(&gen->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    set(mhcudaRuntimeError);
+    return nullptr;
+  }
+  const size_t table = static_cast<size_t>(dim) * 3 * gen->s_pad * sizeof(float);
+  if (cudaMalloc(&gen->params, table) != cudaSuccess) {
+    cudaGetLastError();
+    gen->params = nullptr;
+    MHB_INFO(gen.get(), "failed to allocate %zu bytes for the parameter table\n", table);
+    set(mhcudaMemoryAllocationFailure);
+    return nullptr;
+  }
+  // Zero fill: padding samples and, with `deferred`, the whole table.
+  if (cudaMemsetAsync(gen->params, 0, table, gen->stream) != cudaSuccess) {
+    set(mhcudaRuntimeError);
+    return nullptr;
+  }
+  if (!deferred) {
+    const MHCUDAResult r = init_params(gen.get(), seed);
+    if (r != mhcudaSuccess) {
+      set(r);
+      return nullptr;
+    }
+  }
+  if (cudaStreamSynchronize(gen->stream) != cudaSuccess) {
+    set(mhcudaRuntimeError);
+    return nullptr;
+  }
+  if (verbosity > 1) {
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    printf("GPU #%d memory: used %zu bytes, free %zu bytes, total %zu bytes\n", dev,
+           total_b - free_b, free_b, total_b);
+  }
+  set(mhcudaSuccess);
+  return gen.release();
+}
+
+MinhashCudaGeneratorParameters mhcuda_get_parameters(const MinhashCudaGenerator *gen) {
+  if (!gen) return MinhashCudaGeneratorParameters{};
+  MinhashCudaGeneratorParameters p{};
+  p.dim = gen->dim;
+  p.samples = gen->samples;
+  p.verbosity = gen->verbosity;
+  return p;
+}
+
+enum MHCUDAResult mhcuda_retrieve_random_vars(const MinhashCudaGenerator *gen, float *rs,
+                                              float *ln_cs, float *betas) {
+  if (!gen || !rs || !ln_cs || !betas) return mhcudaInvalidArguments;
+  std::lock_guard<std::mutex> lock(gen->mu);
+  MHB_CHECK(gen, cudaSetDevice(gen->device), mhcudaNoSuchDevice);
+  const size_t n = static_cast<size_t>(gen->dim) * gen->samples;
+  DevBuf tmp;
+  MHB_CHECK(gen, tmp.ensure(n * sizeof(float)), mhcudaMemoryAllocationFailure);
+  float *dst[3] = {rs, ln_cs, betas};
+  for (uint32_t which = 0; which < 3; ++which) {
+    MHB_CHECK(gen, mhb::launch_unpack_params(gen->params, which, gen->dim, gen->samples,
+                                             gen->s_pad, tmp.as<float>(), gen->stream),
+              mhcudaRuntimeError);
+    MHB_CHECK(gen, cudaMemcpyAsync(dst[which], tmp.ptr, n * sizeof(float),
+                                   cudaMemcpyDeviceToHost, gen->stream),
+              mhcudaMemoryCopyError);
+    MHB_CHECK(gen, cudaStreamSynchronize(gen->stream), mhcudaMemoryCopyError);
+  }
+  return mhcudaSuccess;
+}
+
+enum MHCUDAResult mhcuda_assign_random_vars(const MinhashCudaGenerator *gen, const float *rs,
+                                            const float *ln_cs, const float *betas) {
+  if (!gen || !rs || !ln_cs || !betas) return mhcudaInvalidArguments;
+  std::lock_guard<std::mutex> lock(gen->mu);
+  MHB_CHECK(gen, cudaSetDevice(gen->device), mhcudaNoSuchDevice);
+  const size_t n = static_cast<size_t>(gen->dim) * gen->samples;
+  DevBuf tmp;
+  MHB_CHECK(gen, tmp.ensure(n * sizeof(float)), mhcudaMemoryAllocationFailure);
+  const float *src[3] = {rs, ln_cs, betas};
+  for (uint32_t which = 0; which < 3; ++which) {
+    MHB_CHECK(gen, cudaMemcpyAsync(tmp.ptr, src[which], n * sizeof(float),
+                                   cudaMemcpyHostToDevice, gen->stream),
+              mhcudaMemoryCopyError);
+    MHB_CHECK(gen, mhb::launch_pack_params(tmp.as<float>(), nullptr, mhb::PairOp::kCopy, which,
+                                           gen->dim, gen->samples, gen->s_pad, gen->params,
+                                           gen->stream),
+              mhcudaRuntimeError);
+    MHB_CHECK(gen, cudaStreamSynchronize(gen->stream), mhcudaMemoryCopyError);
+  }
+  return mhcudaSuccess;
+}
+
+enum MHCUDAResult mhcuda_calc(const MinhashCudaGenerator *gen, const float *weights,
+                              const uint32_t *cols, const uint32_t *rows, uint32_t length,
+                              uint32_t *output) {
+  if (!gen || !weights || !cols || !rows || !output || length == 0) return mhcudaInvalidArguments;
+  std::lock_guard<std::mutex> lock(gen->mu);
+  MHB_CHECK(gen, cudaSetDevice(gen->device), mhcudaNoSuchDevice);
+  const uint32_t base = rows[0];
+  if (rows[length] < base) return mhcudaInvalidArguments;
+  const uint32_t nnz = rows[length] - base;
+  const cudaStream_t st = gen->stream;
+  MHB_CHECK(gen, gen->d_weights.ensure(static_cast<size_t>(nnz) * 4 + 16),
+            mhcudaMemoryAllocationFailure);
+  MHB_CHECK(gen, gen->d_cols.ensure(static_cast<size_t>(nnz) * 4 + 16),
+            mhcudaMemoryAllocationFailure);
+  MHB_CHECK(gen, gen->d_indptr.ensure((static_cast<size_t>(length) + 1) * 4),
+            mhcudaMemoryAllocationFailure);
+  const size_t out_bytes = static_cast<size_t>(length) * gen->samples * 2 * sizeof(uint32_t);
+  MHB_CHECK(gen, gen->d_out.ensure(out_bytes), mhcudaMemoryAllocationFailure);
+  MHB_INFO(gen, "Preparing...\n");
+  MHB_CHECK(gen, cudaMemcpyAsync(gen->d_indptr.ptr, rows, (static_cast<size_t>(length) + 1) * 4,
+                                 cudaMemcpyHostToDevice, st),
+            mhcudaMemoryCopyError);
+  if (nnz) {
+    MHB_CHECK(gen, cudaMemcpyAsync(gen->d_weights.ptr, weights + base,
+                                   static_cast<size_t>(nnz) * 4, cudaMemcpyHostToDevice, st),
+              mhcudaMemoryCopyError);
+    MHB_CHECK(gen, cudaMemcpyAsync(gen->d_cols.ptr, cols + base, static_cast<size_t>(nnz) * 4,
+                                   cudaMemcpyHostToDevice, st),
+              mhcudaMemoryCopyError);
+  }
+  const HashPlan plan = make_plan(gen, nnz, length);
+  HashArgs a{};
+  MHCUDAResult r = prepare_launch(gen, length, nnz, plan, &a);
+  if (r != mhcudaSuccess) return r;
+  a.weights = gen->d_weights.as<float>();
+  a.cols = gen->d_cols.as<uint32_t>();
+  a.indptr = gen->d_indptr.as<uint32_t>();
+  a.out = gen->d_out.as<uint32_t>();
+  MHB_DEBUG(gen, "plan: spl=%u tiles=%u chunk=%u chunks=%u grid=%u\n", plan.spl, plan.ntiles,
+            plan.chunk, plan.nchunks, plan.grid);
+  MHB_INFO(gen, "Executing the CUDA kernel...\n");
+  r = enqueue_hash(gen, a, plan, st);
+  if (r != mhcudaSuccess) return r;
+  MHB_CHECK(gen, cudaMemcpyAsync(output, gen->d_out.ptr, out_bytes, cudaMemcpyDeviceToHost, st),
+            mhcudaMemoryCopyError);
+  r = read_status(gen, st);
+  if (r != mhcudaSuccess) return r;
+  MHB_INFO(gen, "mhcuda - success\n");
+  return mhcudaSuccess;
+}
+
+enum MHCUDAResult mhcuda_calc_device(const MinhashCudaGenerator *gen, const float *d_weights,
+                                     const uint32_t *d_cols, const uint32_t *d_rows,
+                                     uint32_t length, uint32_t nnz, uint32_t *d_output,
+                                     void *stream) {
+  if (!gen || !d_rows || !d_output || length == 0 || (nnz && (!d_weights || !d_cols)))
+    return mhcudaInvalidArguments;
+  std::lock_guard<std::mutex> lock(gen->mu);
+  MHB_CHECK(gen, cudaSetDevice(gen->device), mhcudaNoSuchDevice);
+  const cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : gen->stream;
+  const HashPlan plan = make_plan(gen, nnz, length);
+  HashArgs a{};
+  MHCUDAResult r = prepare_launch(gen, length, nnz, plan, &a);
+  if (r != mhcudaSuccess) return r;
+  a.weights = d_weights;
+  a.cols = d_cols;
+  a.indptr = d_rows;
+  a.out = d_output;
+  return enqueue_hash(gen, a, plan, st);
+}
+
+enum MHCUDAResult mhcuda_device_status(const MinhashCudaGenerator *gen) {
+  if (!gen) return mhcudaInvalidArguments;
+  std::lock_guard<std::mutex> lock(gen->mu);
+  MHB_CHECK(gen, cudaSetDevice(gen->device), mhcudaNoSuchDevice);
+  MHB_CHECK(gen, cudaDeviceSynchronize(), mhcudaRuntimeError);
+  if (!gen->d_status.ptr) return mhcudaSuccess;
+  const MHCUDAResult r = read_status(gen, gen->stream);
+  MHB_CHECK(gen, cudaMemset(gen->d_status.ptr, 0, sizeof(uint32_t)), mhcudaRuntimeError);
+  return r;
+}
+
+enum MHCUDAResult mhcuda_calc_batch(const MinhashCudaGenerator *gen, uint32_t count,
+                                    const float *const *weights, const uint32_t *const *cols,
+                                    const uint32_t *const *rows, const uint32_t *lengths,
+                                    uint32_t *const *outputs) {
+  if (!gen || !weights || !cols || !rows || !lengths || !outputs) return mhcudaInvalidArguments;
+  std::lock_guard<std::mutex> lock(gen->mu);
+  MHB_CHECK(gen, cudaSetDevice(gen->device), mhcudaNoSuchDevice);
+  // Global row / position offsets of each matrix in the staged batch.
+  std::vector<uint64_t> row_off(count + 1, 0), pos_off(count + 1, 0);
+  for (uint32_t i = 0; i < count; ++i) {
+    uint64_t len = lengths[i], n = 0;
+    if (len) {
+      if (!weights[i] || !cols[i] || !rows[i] || !outputs[i]) return mhcudaInvalidArguments;
+      if (rows[i][len] < rows[i][0]) return mhcudaInvalidArguments;
+      n = rows[i][len] - rows[i][0];
+    }
+    row_off[i + 1] = row_off[i] + len;
+    pos_off[i + 1] = pos_off[i] + n;
+  }
+  const uint64_t total_rows = row_off[count], total_nnz = pos_off[count];
+  if (total_rows == 0) return mhcudaSuccess;
+  if (total_rows >= 0xFFFFFFFFull || total_nnz >= 0xFFFFFFFFull) return mhcudaInvalidArguments;
+  const cudaStream_t st = gen->stream;
+  // Pinned staging: weights | cols | indptr, gathered by a few host threads.
+  const size_t wb = total_nnz * 4, ib = (total_rows + 1) * 4;
+  MHB_CHECK(gen, gen->h_stage.ensure(2 * wb + ib), mhcudaMemoryAllocationFailure);
+  char *stage = gen->h_stage.as<char>();
+  float *sw = reinterpret_cast<float *>(stage);
+  uint32_t *sc = reinterpret_cast<uint32_t *>(stage + wb);
+  uint32_t *si = reinterpret_cast<uint32_t *>(stage + 2 * wb);
+  const unsigned nth = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+  {
+    std::vector<std::thread> pool;
+    for (unsigned t = 0; t < nth; ++t) {
+      pool.emplace_back([&, t]() {
+        for (uint32_t i = t; i < count; i += nth) {
+          const uint64_t len = lengths[i];
+          if (!len) continue;
+          const uint32_t b = rows[i][0];
+          const uint64_t n = pos_off[i + 1] - pos_off[i];
+          memcpy(sw + pos_off[i], weights[i] + b, n * 4);
+          memcpy(sc + pos_off[i], cols[i] + b, n * 4);
+          for (uint64_t r = 0; r < len; ++r)
+            si[row_off[i] + r] = static_cast<uint32_t>(pos_off[i] + (rows[i][r] - b));
+        }
+      });
+    }
+    for (auto &th : pool) th.join();
+  }
+  si[total_rows] = static_cast<uint32_t>(total_nnz);
+  const uint32_t nnz = static_cast<uint32_t>(total_nnz), R = static_cast<uint32_t>(total_rows);
+  MHB_CHECK(gen, gen->d_weights.ensure(wb + 16), mhcudaMemoryAllocationFailure);
+  MHB_CHECK(gen, gen->d_cols.ensure(wb + 16), mhcudaMemoryAllocationFailure);
+  MHB_CHECK(gen, gen->d_indptr.ensure(ib), mhcudaMemoryAllocationFailure);
+  const size_t row_bytes = static_cast<size_t>(gen->samples) * 2 * sizeof(uint32_t);
+  MHB_CHECK(gen, gen->d_out.ensure(total_rows * row_bytes), mhcudaMemoryAllocationFailure);
+  if (wb) {
+    MHB_CHECK(gen, cudaMemcpyAsync(gen->d_weights.ptr, sw, wb, cudaMemcpyHostToDevice, st),
+              mhcudaMemoryCopyError);
+    MHB_CHECK(gen, cudaMemcpyAsync(gen->d_cols.ptr, sc, wb, cudaMemcpyHostToDevice, st),
+              mhcudaMemoryCopyError);
+  }
+  MHB_CHECK(gen, cudaMemcpyAsync(gen->d_indptr.ptr, si, ib, cudaMemcpyHostToDevice, st),
+            mhcudaMemoryCopyError);
+  const HashPlan plan = make_plan(gen, nnz, R);
+  HashArgs a{};
+  MHCUDAResult r = prepare_launch(gen, R, nnz, plan, &a);
+  if (r != mhcudaSuccess) return r;
+  a.weights = gen->d_weights.as<float>();
+  a.cols = gen->d_cols.as<uint32_t>();
+  a.indptr = gen->d_indptr.as<uint32_t>();
+  a.out = gen->d_out.as<uint32_t>();
+  r = enqueue_hash(gen, a, plan, st);
+  if (r != mhcudaSuccess) return r;
+  for (uint32_t i = 0; i < count; ++i) {
+    if (!lengths[i]) continue;
+    MHB_CHECK(gen, cudaMemcpyAsync(outputs[i], gen->d_out.as<char>() + row_off[i] * row_bytes,
+                                   lengths[i] * row_bytes, cudaMemcpyDeviceToHost, st),
+              mhcudaMemoryCopyError);
+  }
+  return read_status(gen, st);
+}
+
+enum MHCUDAResult mhcuda_debug_device_logf(uint32_t devices, const float *in, float *out,
+                                           uint64_t n) {
+  if (!in || !out) return mhcudaInvalidArguments;
+  const int dev = pick_device(devices);
+  if (dev < 0 || cudaSetDevice(dev) != cudaSuccess) {
+    cudaGetLastError();
+    return mhcudaNoSuchDevice;
+  }
+  if (n == 0) return mhcudaSuccess;
+  DevBuf a, b;
+  if (a.ensure(n * 4) != cudaSuccess || b.ensure(n * 4) != cudaSuccess)
+    return mhcudaMemoryAllocationFailure;
+  if (cudaMemcpy(a.ptr, in, n * 4, cudaMemcpyHostToDevice) != cudaSuccess)
+    return mhcudaMemoryCopyError;
+  if (mhb::launch_logf(a.as<float>(), b.as<float>(), n, nullptr) != cudaSuccess)
+    return mhcudaRuntimeError;
+  if (cudaMemcpy(out, b.ptr, n * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return mhcudaMemoryCopyError;
+  return mhcudaSuccess;
+}
+
+enum MHCUDAResult mhcuda_profile(const MinhashCudaGenerator *gen, int enable) {
+  if (!gen) return mhcudaInvalidArguments;
+  std::lock_guard<std::mutex> lock(gen->mu);
+  gen->profiling = enable != 0;
+  gen->prof_used = 0;
+  return mhcudaSuccess;
+}
+
+enum MHCUDAResult mhcuda_profile_read(const MinhashCudaGenerator *gen, double *hash_ms,
+                                      uint64_t *launches) {
+  if (!gen || !hash_ms || !launches) return mhcudaInvalidArguments;
+  std::lock_guard<std::mutex> lock(gen->mu);
+  MHB_CHECK(gen, cudaSetDevice(gen->device), mhcudaNoSuchDevice);
+  double total = 0.0;
+  for (size_t i = 0; i < gen->prof_used; ++i) {
+    MHB_CHECK(gen, cudaEventSynchronize(gen->prof_events[i].second), mhcudaRuntimeError);
+    float ms = 0.0f;
+    MHB_CHECK(gen, cudaEventElapsedTime(&ms, gen->prof_events[i].first,
+                                        gen->prof_events[i].second),
+              mhcudaRuntimeError);
+    total += ms;
+  }
+  *hash_ms = total;
+  *launches = gen->prof_used;
+  gen->prof_used = 0;
+  return mhcudaSuccess;
+}
+
+enum MHCUDAResult mhcuda_fini(MinhashCudaGenerator *gen) {
+  delete gen;
+  return mhcudaSuccess;
+}
+
+}  // extern "C"

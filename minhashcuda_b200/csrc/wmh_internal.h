@@ -1,0 +1,88 @@
+// Internal declarations shared by the kernels (*.cu) and the host engine.
+// Nothing here is part of the public ABI (include/minhashcuda*.h is).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+namespace mhb {
+
+constexpr uint32_t kNone = 0xFFFFFFFFu;
+
+// Device status word bits (written by kernels, read by the host).
+constexpr uint32_t kStatusBadColumn = 1u;  // a column index >= dim was seen
+constexpr uint32_t kStatusBadIndptr = 2u;  // row offsets decrease or disagree with nnz
+
+// Parameter table: one contiguous block per column d,
+//   params[(d * 3 + 0) * s_pad + s] = r      (rs)
+//   params[(d * 3 + 1) * s_pad + s] = ln_c   (ln_cs)
+//   params[(d * 3 + 2) * s_pad + s] = beta   (betas)
+// s_pad = samples rounded up to a multiple of 4, so every section starts on a
+// 16-byte boundary and a lane can fetch 4 consecutive samples as one float4.
+inline uint32_t padded_samples(uint32_t samples) { return (samples + 3u) & ~3u; }
+
+// Work decomposition of one hash launch.
+//
+// The CSR's nnz positions [0, nnz) (relative to indptr[0]) are cut into
+// `nchunks` chunks of `chunk` positions (a multiple of 32).  A row belongs to
+// the chunk holding its first position (trailing empty rows to the last
+// chunk).  A warp hashes one (chunk, sample-tile) item: it finishes every row
+// that lies inside the chunk and leaves a partial arg-min for the row that
+// runs in from the previous chunk ("head", slot 2c) and for the row that runs
+// out past the chunk's end ("tail", slot 2c+1).  A finalize pass merges the
+// partials of every row that crosses a chunk boundary, earlier positions
+// winning ties exactly as the reference's strict '<' scan does.
+struct HashPlan {
+  uint32_t chunk;    // positions per chunk, multiple of 32
+  uint32_t nchunks;  // >= 1
+  uint32_t spl;      // samples per lane in one item: 1, 2 or 4
+  uint32_t ntiles;   // sample tiles of 32*spl samples
+  uint32_t grid;     // persistent grid (blocks of kHashBlock threads)
+};
+
+constexpr int kHashBlock = 256;
+
+struct HashArgs {
+  const float *params;       // [dim][3][s_pad]
+  uint32_t dim;
+  uint32_t samples;
+  uint32_t s_pad;
+  const float *weights;      // CSR values, weights[p] for relative position p
+  const uint32_t *cols;      // CSR column indices
+  const uint32_t *indptr;    // rows+1 absolute offsets, indptr[0] = base
+  uint32_t rows;
+  uint32_t nnz;              // indptr[rows] - indptr[0]
+  uint32_t chunk;
+  uint32_t nchunks;
+  uint32_t ntiles;
+  uint32_t *chunk_row;       // [nchunks] first row owned by each chunk
+  float *part_ln;            // [2*nchunks][s_pad] partial minima
+  uint2 *part_kt;            // [2*nchunks][s_pad] partial (k, float bits of t)
+  uint32_t *out;             // [rows][samples][2]
+  uint32_t *status;          // device status word
+};
+
+// Launchers (hash_kernels.cu).  All enqueue on `stream` and return the launch
+// error, if any.
+cudaError_t launch_plan(const HashArgs &a, cudaStream_t stream);
+cudaError_t launch_hash(const HashArgs &a, const HashPlan &plan, cudaStream_t stream);
+cudaError_t launch_finalize(const HashArgs &a, cudaStream_t stream);
+// Blocks per SM the hash kernel reaches for a given samples-per-lane value.
+int hash_blocks_per_sm(uint32_t spl);
+size_t hash_kernel_registers(uint32_t spl);
+
+// Parameter kernels (param_kernels.cu).
+enum class PairOp : int { kGamma = 0, kLogGamma = 1, kCopy = 2 };
+// params[d][which][s] = op(a[s*dim + d], b[s*dim + d]) for s < samples.
+cudaError_t launch_pack_params(const float *a, const float *b, PairOp op, uint32_t which,
+                               uint32_t dim, uint32_t samples, uint32_t s_pad,
+                               float *params, cudaStream_t stream);
+// dst[s*dim + d] = params[d][which][s].
+cudaError_t launch_unpack_params(const float *params, uint32_t which, uint32_t dim,
+                                 uint32_t samples, uint32_t s_pad, float *dst,
+                                 cudaStream_t stream);
+cudaError_t launch_logf(const float *in, float *out, size_t n, cudaStream_t stream);
+
+}  // namespace mhb

@@ -1,0 +1,173 @@
+"""Engine vs oracle through the C ABI on a B200: bit-exact hashes.
+
+The oracle is fed the GPU's own logf of every weight (mhcuda_debug_device_logf)
+so the comparison is exact by construction; every other operation is
+correctly rounded on both sides.
+"""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+import oracle as O
+from wmh_testlib import device_logf, engine_gen, gamma_params, random_csr
+
+pytestmark = pytest.mark.gpu
+
+
+def check(m, samples, params, **calc_kw):
+    dim = m.shape[1]
+    with engine_gen(dim, samples, deferred=True) as eng:
+        eng.assign(*params)
+        out = eng.calc_csr(m)
+    want = O.COracle(*params).hash_csr(m, lnw=device_logf(m.data))
+    np.testing.assert_array_equal(out, want)
+    return out
+
+
+@pytest.mark.parametrize("samples", [1, 2, 3, 5, 17, 31, 32, 33, 64, 100, 127, 128, 129, 200,
+                                     256, 300, 512, 1000])
+def test_samples_sweep(samples):
+    rng = np.random.default_rng(samples)
+    dim = 700
+    m = random_csr(rng, 300, dim, 25, empty_frac=0.03)
+    check(m, samples, gamma_params(rng, dim, samples))
+
+
+@pytest.mark.parametrize("mean_nnz", [1, 3, 30, 200, 1500])
+def test_row_length_sweep(mean_nnz):
+    rng = np.random.default_rng(mean_nnz)
+    dim = 4000
+    m = random_csr(rng, 400, dim, mean_nnz)
+    check(m, 128, gamma_params(rng, dim, 128))
+
+
+def test_long_rows_cross_many_chunks():
+    """Rows far longer than a chunk are merged across chunks in position order."""
+    rng = np.random.default_rng(9)
+    dim = 60000
+    m = random_csr(rng, 50, dim, 10, long_rows=[(0, 50000), (7, 20000), (49, 33333)])
+    check(m, 128, gamma_params(rng, dim, 128))
+    check(m, 64, gamma_params(rng, dim, 64))
+
+
+def test_empty_zero_negative_nan_rows():
+    rng = np.random.default_rng(4)
+    dim = 200
+    m = random_csr(rng, 500, dim, 8, empty_frac=0.2, zero_frac=0.3)
+    d = m.data.copy()
+    d[rng.random(d.size) < 0.05] = -1.0
+    d[rng.random(d.size) < 0.02] = np.nan
+    d[rng.random(d.size) < 0.02] = np.inf
+    m = sp.csr_matrix((d, m.indices, m.indptr), shape=m.shape)
+    out = check(m, 128, gamma_params(rng, dim, 128))
+    empty = np.diff(m.indptr) == 0
+    assert (out[empty] == 0xFFFFFFFF).all()
+
+
+def test_all_rows_empty_and_trailing_empty():
+    rng = np.random.default_rng(1)
+    dim = 50
+    params = gamma_params(rng, dim, 32)
+    m = sp.csr_matrix((5, dim), dtype=np.float32)
+    out = check(m, 32, params)
+    assert (out == 0xFFFFFFFF).all()
+    m = random_csr(rng, 40, dim, 5)
+    ip = np.concatenate([m.indptr, [m.indptr[-1]] * 7])
+    m2 = sp.csr_matrix((m.data, m.indices, ip), shape=(47, dim))
+    out = check(m2, 32, params)
+    assert (out[40:] == 0xFFFFFFFF).all()
+
+
+def test_duplicate_columns_and_ties():
+    """Duplicate columns inside a row and identical parameters across columns:
+    the first entry in storage order wins (strict '<', kernel.cu:106)."""
+    dim, samples = 16, 64
+    rng = np.random.default_rng(2)
+    rs, lc, b = gamma_params(rng, dim, samples)
+    rs[:, 5] = rs[:, 9]
+    lc[:, 5] = lc[:, 9]
+    b[:, 5] = b[:, 9]
+    data = np.array([3.0, 3.0, 2.0, 2.0, 7.0, 7.0], np.float32)
+    cols = np.array([9, 5, 4, 4, 1, 1], np.uint32)
+    ip = np.array([0, 2, 4, 6])
+    m = sp.csr_matrix((data, cols, ip), shape=(3, dim))
+    out = check(m, samples, (rs, lc, b))
+    assert (out[0, :, 0] == 9).all()
+
+
+def test_unsorted_columns():
+    rng = np.random.default_rng(8)
+    dim = 900
+    m = random_csr(rng, 300, dim, 40, sort_cols=False)
+    check(m, 128, gamma_params(rng, dim, 128))
+
+
+def test_invalid_column_is_rejected():
+    rng = np.random.default_rng(0)
+    dim = 10
+    with engine_gen(dim, 16, seed=1) as eng:
+        rc, _ = eng.calc_raw(np.ones(3, np.float32), np.array([1, 10, 2], np.uint32),
+                             np.array([0, 3], np.uint32))
+        assert rc == 1  # mhcudaInvalidArguments
+        # The generator stays usable.
+        out = eng.calc(np.ones(2, np.float32), np.array([1, 2], np.uint32),
+                       np.array([0, 2], np.uint32))
+        assert out.shape == (1, 16, 2)
+    del rng
+
+
+def test_decreasing_offsets_are_rejected():
+    with engine_gen(10, 16, seed=1) as eng:
+        rc, _ = eng.calc_raw(np.ones(4, np.float32), np.array([1, 2, 3, 4], np.uint32),
+                             np.array([0, 3, 2, 4], np.uint32))
+        assert rc == 1
+        rc, _ = eng.calc_raw(np.ones(1, np.float32), np.array([1], np.uint32),
+                             np.array([0, 1], np.uint32), length=0)
+        assert rc == 1
+
+
+def test_repeated_calls_reuse_buffers():
+    """Grow-only workspace: a large call followed by smaller ones (and back)."""
+    rng = np.random.default_rng(12)
+    dim = 3000
+    params = gamma_params(rng, dim, 128)
+    co = O.COracle(*params)
+    with engine_gen(dim, 128, deferred=True) as eng:
+        eng.assign(*params)
+        for rows, nnz in ((2000, 100), (3, 5), (500, 400), (1, 1), (2500, 50)):
+            m = random_csr(rng, rows, dim, nnz)
+            np.testing.assert_array_equal(eng.calc_csr(m),
+                                          co.hash_csr(m, lnw=device_logf(m.data)))
+
+
+def test_rows_offset_is_absolute():
+    rng = np.random.default_rng(13)
+    dim = 400
+    params = gamma_params(rng, dim, 128)
+    m = random_csr(rng, 100, dim, 30)
+    with engine_gen(dim, 128, deferred=True) as eng:
+        eng.assign(*params)
+        full = eng.calc_csr(m)
+        part = eng.calc(m.data, m.indices, m.indptr[20:61])
+    np.testing.assert_array_equal(part, full[20:60])
+
+
+def test_batch_equals_plain_calls():
+    import minhashcuda_b200
+    from minhashcuda_b200 import libMHCUDA as L
+    rng = np.random.default_rng(14)
+    dim = 2048
+    params = gamma_params(rng, dim, 256)
+    mats = [random_csr(rng, int(rng.integers(1, 300)), dim, float(rng.integers(1, 80)))
+            for _ in range(40)]
+    gen = L.minhash_cuda_init(dim, 256, deferred=True)
+    try:
+        L.minhash_cuda_assign_vars(gen, *params)
+        batch = L.minhash_cuda_calc_batch(gen, mats)
+        plain = [L.minhash_cuda_calc(gen, m) for m in mats]
+    finally:
+        L.minhash_cuda_fini(gen)
+    assert len(batch) == len(mats)
+    for b, p in zip(batch, plain):
+        np.testing.assert_array_equal(b, p)
+    del minhashcuda_b200

@@ -1,0 +1,147 @@
+"""The reference itself, built from its own sources for sm_100a
+(oracle/Makefile `ref` -> oracle/_ref/libMHCUDA.so), run on the same B200 as
+the engine.  These tests pin the oracle and the engine to the reference:
+
+  * which float form the reference build evaluates kernel.cu:104-105 in
+    (crafted near-tie inputs where the fused and unfused forms pick different
+    columns),
+  * the cuRAND parameter stream: equal seeds give bit-equal rs/ln_cs/betas,
+  * hash outputs: bit-equal on every (row, sample) the reference defines.
+
+Cells without any selectable entry are undefined in the reference (it writes
+stale memory, kernel.cu:81-87) and are excluded.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from wmh_testlib import (CGen, device_logf, engine_gen, gamma_params, random_csr, reference_lib,
+                         selected)
+
+
+def crafted_form_case(rng, rows=16, samples=64):
+    """Rows of two entries (columns 2i, 2i+1, equal weights) whose params make
+    the fused and unfused evaluation of ln_a order the two entries
+    differently, in (almost) every sample."""
+    import scipy.sparse as sp
+    dim = 2 * rows
+    rs = np.ones((samples, dim), np.float32)
+    lc = np.zeros((samples, dim), np.float32)
+    b = np.zeros((samples, dim), np.float32)
+    w = rng.uniform(-4, 4, rows).astype(np.float32)
+    weights = np.exp(w.astype(np.float64)).astype(np.float32)
+    lnw = np.log(weights)  # host log; the GPU's may differ by an ulp -> recomputed below
+    M = 256
+    for i in range(rows):
+        for s in range(samples):
+            r = rng.uniform(0.05, 6, M).astype(np.float32)
+            beta = rng.uniform(0, 1, M).astype(np.float32)
+            ca = rng.uniform(-3, 3, M).astype(np.float32)
+            k = rng.integers(-3, 4, M)
+            cb = (ca.view(np.int32) + k.astype(np.int32)).view(np.float32)
+            with np.errstate(all="ignore"):
+                t = np.floor(lnw[i] / r + beta)
+                tb = t - beta
+                prod = tb.astype(np.float64) * r.astype(np.float64)
+                fa = O._round_odd_sub_to_f32(ca.astype(np.float64), prod) - r
+                fb = O._round_odd_sub_to_f32(cb.astype(np.float64), prod) - r
+                ua = (ca - tb * r) - r
+                ub = (cb - tb * r) - r
+            differ = (fb < fa) != (ub < ua)
+            j = int(np.argmax(differ)) if differ.any() else 0
+            rs[s, 2 * i] = rs[s, 2 * i + 1] = r[j]
+            b[s, 2 * i] = b[s, 2 * i + 1] = beta[j]
+            lc[s, 2 * i], lc[s, 2 * i + 1] = ca[j], cb[j]
+    cols = np.arange(dim, dtype=np.uint32)
+    indptr = np.arange(0, dim + 1, 2, dtype=np.int64)
+    data = np.repeat(weights, 2)
+    return rs, lc, b, sp.csr_matrix((data, cols, indptr), shape=(rows, dim))
+
+
+def _ref_gen(dim, samples, seed=1, deferred=False):
+    lib = reference_lib()
+    if lib is None:
+        pytest.skip("reference build oracle/_ref/libMHCUDA.so not present")
+    return CGen(lib, dim, samples, seed=seed, deferred=deferred, devices=1)
+
+
+@pytest.mark.gpu
+def test_reference_fma_form():
+    """The reference build contracts ln_c - (t-beta)*r into one FMA, and the
+    engine and the oracle's REFERENCE_FORM do the same."""
+    rng = np.random.default_rng(11)
+    rs, lc, b, m = crafted_form_case(rng, rows=16, samples=64)
+    lnw = device_logf(m.data)
+    co = O.COracle(rs, lc, b)
+    fused = co.hash_csr(m, form=O.FORM_FUSED, lnw=lnw)
+    unfused = co.hash_csr(m, form=O.FORM_UNFUSED, lnw=lnw)
+    differ = (fused != unfused).any(axis=2)
+    assert differ.mean() > 0.9
+    with _ref_gen(m.shape[1], 64, deferred=True) as ref:
+        ref.assign(rs, lc, b)
+        rout = ref.calc_csr(m)
+    match_fused = (rout == fused).all(axis=2)[differ].mean()
+    match_unfused = (rout == unfused).all(axis=2)[differ].mean()
+    print(f"reference matches fused on {match_fused:.4f}, unfused on {match_unfused:.4f} "
+          f"of {differ.sum()} separating cells")
+    expected = fused if O.REFERENCE_FORM == O.FORM_FUSED else unfused
+    np.testing.assert_array_equal(rout, expected)
+    with engine_gen(m.shape[1], 64, deferred=True) as eng:
+        eng.assign(rs, lc, b)
+        np.testing.assert_array_equal(eng.calc_csr(m), expected)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dim,samples,seed", [(130, 128, 1), (1000, 128, 7), (23, 128, 0),
+                                              (4096, 64, 3), (777, 256, 42)])
+def test_curand_parameter_parity(dim, samples, seed):
+    """Same seed -> the same cuRAND draws and the same float ops as
+    minhashcuda.cc:179-200 / kernel.cu:18-36: bit-equal parameters."""
+    with _ref_gen(dim, samples, seed=seed) as ref:
+        want = ref.retrieve()
+    with engine_gen(dim, samples, seed=seed) as eng:
+        got = eng.retrieve()
+    for name, g, w in zip(("rs", "ln_cs", "betas"), got, want):
+        np.testing.assert_array_equal(g.view(np.uint32), w.view(np.uint32), err_msg=name)
+
+
+def _compare_with_reference(m, samples, params=None, seed=1):
+    dim = m.shape[1]
+    with _ref_gen(dim, samples, seed=seed, deferred=params is not None) as ref:
+        if params is not None:
+            ref.assign(*params)
+        rout = ref.calc_csr(m)
+        rparams = ref.retrieve()
+    with engine_gen(dim, samples, deferred=True) as eng:
+        eng.assign(*rparams)
+        eout = eng.calc_csr(m)
+    mask = selected(eout)
+    np.testing.assert_array_equal(eout[mask], rout[mask])
+    # The engine's undefined cells hold the sentinel; the oracle agrees.
+    co = O.COracle(*rparams)
+    np.testing.assert_array_equal(co.hash_csr(m, lnw=device_logf(m.data)), eout)
+    return mask.mean()
+
+
+@pytest.mark.gpu
+def test_reference_small_config_seeded():
+    """6400x130, seed 1 (test.py:92-101 / README.md:85-98)."""
+    _, m = O.reference_small_matrix(1)
+    frac = _compare_with_reference(m, 128, seed=1)
+    assert frac > 0.99
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("samples", [2, 64, 128, 256])
+def test_reference_random_lognormal(samples):
+    rng = np.random.default_rng(samples)
+    m = random_csr(rng, 3000, 5000, 60, long_rows=[(5, 4000), (1700, 2500)])
+    params = gamma_params(rng, 5000, samples)
+    _compare_with_reference(m, samples, params=params)
+
+
+@pytest.mark.gpu
+def test_reference_integer_weights_with_zeros():
+    rng = np.random.default_rng(3)
+    m = random_csr(rng, 2000, 300, 40, values="int", zero_frac=0.1)
+    _compare_with_reference(m, 128, params=gamma_params(rng, 300, 128))
