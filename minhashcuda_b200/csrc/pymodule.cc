@@ -9,8 +9,10 @@
 //   mhcudaMemoryCopyError         -> RuntimeError
 //   mhcudaRuntimeError            -> AssertionError
 // Additions: minhash_cuda_assign_random_vars (alias of minhash_cuda_assign_vars,
-// the name README.md:125 uses), minhash_cuda_calc_batch, and acceptance of
-// scipy.sparse.csr_array besides csr_matrix.
+// the name README.md:125 uses), minhash_cuda_calc_batch, acceptance of
+// scipy.sparse.csr_array besides csr_matrix, and casting of float64 (or
+// integer) data and parameter arrays to float32 where the reference accepts
+// only what numpy casts safely.
 #define PY_SSIZE_T_CLEAN
 #include <Python.h>
 #define NPY_NO_DEPRECATED_API NPY_1_7_API_VERSION
@@ -120,7 +122,8 @@ bool is_csr(PyObject *m) {
 bool csr_view(PyObject *m, Csr *out) {
   if (!is_csr(m)) return false;
   Ref d(PyObject_GetAttrString(m, "data"));
-  if (d) out->data = Ref(PyArray_FROM_OTF(d.get(), NPY_FLOAT32, NPY_ARRAY_IN_ARRAY));
+  if (d)
+    out->data = Ref(PyArray_FROM_OTF(d.get(), NPY_FLOAT32, NPY_ARRAY_FORCECAST | NPY_ARRAY_IN_ARRAY));
   if (!out->data) {
     PyErr_SetString(PyExc_ValueError, "Failed to convert csr_matrix.data to numpy.array");
     return false;
@@ -199,7 +202,7 @@ PyObject *py_assign_vars(PyObject *, PyObject *args) {
   Ref arrs[3];
   const float *ptrs[3];
   for (int i = 0; i < 3; ++i) {
-    arrs[i] = Ref(PyArray_FROM_OTF(objs[i], NPY_FLOAT32, NPY_ARRAY_IN_ARRAY));
+    arrs[i] = Ref(PyArray_FROM_OTF(objs[i], NPY_FLOAT32, NPY_ARRAY_FORCECAST | NPY_ARRAY_IN_ARRAY));
     if (!arrs[i]) {
       PyErr_Format(PyExc_ValueError, "Failed to convert %s to numpy array", names[i]);
       return nullptr;

@@ -41,51 +41,87 @@ constexpr int kZipfThreads = 256;
 constexpr int kZipfTable = 4096;  // hash-set slots (power of two)
 constexpr int kZipfMaxRow = 2048; // longest row the Zipf generator fills
 
+__device__ __forceinline__ uint32_t slot_of(uint32_t col) {
+  return static_cast<uint32_t>(mix64(col) & (kZipfTable - 1));
+}
+
 __global__ void zipf_cols_kernel(uint32_t rows, uint64_t row0, const uint32_t *__restrict__ indptr,
-                                 uint32_t dim, double s, uint64_t seed, uint64_t perm_a, uint64_t perm_b,
-                                 uint32_t *__restrict__ cols, uint32_t *__restrict__ status) {
-  __shared__ uint32_t table[kZipfTable];
+                                 uint32_t dim, double s, uint64_t seed, uint64_t perm_a,
+                                 uint64_t perm_b, uint32_t *__restrict__ cols,
+                                 uint32_t *__restrict__ status) {
+  __shared__ uint32_t table[kZipfTable];  // col + 1, 0 = empty (linear probing)
+  __shared__ uint32_t owner[kZipfTable];  // lowest thread that drew the slot's col this round
   __shared__ uint32_t list[kZipfMaxRow];
+  __shared__ uint32_t warp_new[kZipfThreads / 32];
   __shared__ uint32_t count;
+  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
   const double one_minus_s = 1.0 - s;
   const double top = pow(static_cast<double>(dim) + 1.0, one_minus_s);
   for (uint32_t row = blockIdx.x; row < rows; row += gridDim.x) {
     const uint32_t start = indptr[row];
     const uint32_t n = indptr[row + 1] - start;
     if (n > kZipfMaxRow || n > dim) {
-      if (threadIdx.x == 0) atomicOr(status, 1u);
+      if (tid == 0) atomicOr(status, 1u);
       continue;
     }
-    for (int i = threadIdx.x; i < kZipfTable; i += kZipfThreads) table[i] = 0;
-    if (threadIdx.x == 0) count = 0;
+    for (int i = tid; i < kZipfTable; i += kZipfThreads) {
+      table[i] = 0;
+      owner[i] = 0xFFFFFFFFu;
+    }
+    if (tid == 0) count = 0;
     __syncthreads();
+    // Draw rounds.  A round's new columns are accepted in the order of the
+    // lowest thread that drew each of them, so the row's column set is a
+    // pure function of (seed, row) regardless of atomic ordering.
     for (uint32_t round = 0;; ++round) {
-      // Every thread takes the same snapshot of `count` between two barriers,
-      // so all of them leave the loop in the same round.
-      const uint32_t have = count;
+      const uint32_t have = count;  // same snapshot in every thread
       __syncthreads();
       if (have >= n) break;
       if (round > 100000) {  // cannot happen for n <= dim; keeps the loop finite
-        if (threadIdx.x == 0) atomicOr(status, 2u);
+        if (tid == 0) atomicOr(status, 2u);
         break;
       }
-      const double u = unit(seed, ((row0 + row) << 20) ^ round, threadIdx.x);
+      const double u = unit(seed, ((row0 + row) << 20) ^ round, tid);
       const double x = pow(1.0 - u * (1.0 - top), 1.0 / one_minus_s);
       uint64_t rank = static_cast<uint64_t>(x) - 1;  // [0, dim)
       if (rank >= dim) rank = dim - 1;
       const uint32_t col = static_cast<uint32_t>((perm_a * rank + perm_b) % dim);
       const uint32_t key = col + 1u;
-      uint32_t h = static_cast<uint32_t>(mix64(col) & (kZipfTable - 1));
+      // Phase 1: is the column already in the row (from earlier rounds)?
+      bool old = false;
+      uint32_t h = slot_of(col);
       for (int probe = 0; probe < kZipfTable; ++probe) {
-        const uint32_t old = atomicCAS(&table[h], 0u, key);
-        if (old == 0u) {
-          const uint32_t pos = atomicAdd(&count, 1u);
-          if (pos < n) list[pos] = col;
-          break;
-        }
-        if (old == key) break;
+        const uint32_t v = table[h];
+        if (v == key) { old = true; break; }
+        if (v == 0u) break;
         h = (h + 1) & (kZipfTable - 1);
       }
+      __syncthreads();
+      // Phase 2: insert new columns; every drawer of a column learns its slot.
+      if (!old) {
+        h = slot_of(col);
+        for (int probe = 0; probe < kZipfTable; ++probe) {
+          const uint32_t prev = atomicCAS(&table[h], 0u, key);
+          if (prev == 0u || prev == key) break;
+          h = (h + 1) & (kZipfTable - 1);
+        }
+        atomicMin(&owner[h], tid);
+      }
+      __syncthreads();
+      // Phase 3: the owner of each new column takes a place in thread order.
+      const bool rep = !old && owner[h] == tid;
+      const unsigned ballot = __ballot_sync(0xFFFFFFFFu, rep);
+      if (lane == 0) warp_new[warp] = __popc(ballot);
+      __syncthreads();
+      uint32_t before = __popc(ballot & ((1u << lane) - 1u)), total = 0;
+      for (uint32_t w = 0; w < kZipfThreads / 32; ++w) {
+        if (w < warp) before += warp_new[w];
+        total += warp_new[w];
+      }
+      if (rep && have + before < n) list[have + before] = col;
+      __syncthreads();
+      if (rep) owner[h] = 0xFFFFFFFFu;
+      if (tid == 0) count = min(n, have + total);
       __syncthreads();
     }
     __syncthreads();

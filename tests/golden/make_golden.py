@@ -62,8 +62,8 @@ def main():
     record(args.out, "fma_form_crafted", cm, 64, params=(rs, lc, b))
     # Lognormal weights, a long row, empty rows, 256 samples.
     rng = np.random.default_rng(2024)
-    rm = random_csr(rng, 60, 3000, 25, empty_frac=0.05, long_rows=[(3, 2500)])
-    record(args.out, "lognormal_s256", rm, 256, params=gamma_params(rng, 3000, 256))
+    rm = random_csr(rng, 40, 200, 25, empty_frac=0.05, long_rows=[(3, 190)])
+    record(args.out, "lognormal_s256", rm, 256, params=gamma_params(rng, 200, 256))
 
 
 if __name__ == "__main__":

@@ -136,13 +136,20 @@ def test_float():
 
 def test_split_shapes():
     """test.py:212-232 as intended (its loop is broken as written): unbalanced
-    row lengths, one row each."""
+    row lengths, one row each.  The reference uses mask 4 (device #2 only);
+    like the reference, a mask that names no present device is refused."""
+    import torch
+    mask = 4
+    if torch.cuda.device_count() < 3:
+        with pytest.raises(ValueError, match="No such CUDA device"):
+            libMHCUDA.minhash_cuda_init(10, 128, devices=4)
+        mask = 1
     for v in ([[2], [1], [1], [1]], [[1] * 50, [1], [1], [1]], [[1], [1] * 50, [1], [1]],
               [[1], [1], [1] * 50, [1]], [[1], [1], [1], [1] * 50],
               [[1] * 3, [1] * 10, [1] * 5, [1] * 2]):
         flat = np.array(sum(v, []), dtype=np.float32)
         k = len(flat)
-        gen = libMHCUDA.minhash_cuda_init(k, 128, devices=4, verbosity=2)
+        gen = libMHCUDA.minhash_cuda_init(k, 128, devices=mask, verbosity=2)
         m = sp.csr_matrix(flat[None, :])
         hashes = libMHCUDA.minhash_cuda_calc(gen, m)
         libMHCUDA.minhash_cuda_fini(gen)

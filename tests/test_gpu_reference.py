@@ -145,3 +145,46 @@ def test_reference_integer_weights_with_zeros():
     rng = np.random.default_rng(3)
     m = random_csr(rng, 2000, 300, 40, values="int", zero_frac=0.1)
     _compare_with_reference(m, 128, params=gamma_params(rng, 300, 128))
+
+
+@pytest.mark.gpu
+def test_large_workload_slice_vs_reference_build():
+    """200,000 rows of the benchmark workload (Poisson(1400) nnz, Zipf(1.1)
+    columns over 1M dims, 128 samples, seed 2): the reference build and the
+    engine produce the same hashes through their C ABIs on the same host
+    buffers.  Both calls are timed end to end (host buffers in, hashes out);
+    with MHB_PERF_OUT set the timings are appended there as JSON."""
+    import json
+    import os
+    import time
+    from minhashcuda_b200 import synth
+    w = synth.WORKLOADS["large"]
+    rows = int(os.environ.get("MHB_REF_ROWS", "200000"))
+    ip, cols, wts = synth.host_csr(w, 0, rows)
+    with _ref_gen(w.dim, w.samples, seed=w.seed) as ref:
+        ref.calc(wts, cols, ip[:2])  # warm-up on the first row
+        t0 = time.perf_counter()
+        rout = ref.calc(wts, cols, ip)
+        t_ref = time.perf_counter() - t0
+        params = ref.retrieve()
+    with engine_gen(w.dim, w.samples, seed=w.seed) as eng:
+        got = eng.retrieve()
+        for g, p in zip(got, params):
+            np.testing.assert_array_equal(g.view(np.uint32), p.view(np.uint32))
+        eng.calc(wts, cols, ip[:2])
+        t0 = time.perf_counter()
+        eout = eng.calc(wts, cols, ip)
+        t_eng = time.perf_counter() - t0
+    mask = selected(eout)
+    assert mask.all()
+    np.testing.assert_array_equal(eout, rout)
+    evals = int(ip[-1]) * w.samples
+    rec = {"test": "large_workload_slice", "rows": rows, "nnz": int(ip[-1]),
+           "samples": w.samples, "reference_s": t_ref, "engine_s": t_eng,
+           "reference_evals_per_s": evals / t_ref, "engine_evals_per_s": evals / t_eng,
+           "host_buffers": "pageable numpy"}
+    print(json.dumps(rec))
+    out = os.environ.get("MHB_PERF_OUT")
+    if out:
+        with open(out, "a") as f:
+            f.write(json.dumps(rec) + "\n")
