@@ -16,9 +16,14 @@
 //    32*SPL samples are three fully coalesced warp loads (SPL=4: 3 x 512 B),
 //  - a warp owns one (chunk, sample tile) item; each lane keeps SPL running
 //    minima in registers (no shared-memory spill as in kernel.cu:72-74),
-//  - ln(weight) is evaluated once per nnz, lane-parallel over a 32-entry
-//    block of the CSR (the reference evaluates it once per thread, :95), and
-//    broadcast with warp shuffles,
+//  - each warp stages its CSR positions in 256-entry windows with TMA bulk
+//    copies (cp.async.bulk, mbarrier completion, double-buffered), turns the
+//    weights into ln(weight) in place once per nnz, lane-parallel (the
+//    reference evaluates logf once per thread, :95), and reads them back as
+//    shared-memory broadcasts,
+//  - parameters for the next nnz are loaded into a second register set while
+//    the current one is evaluated (ping-pong, no register copies), and the
+//    running minimum is updated with selects instead of branches,
 //  - work is cut by nnz, not by rows, so one 50k-nnz row and many 5-nnz rows
 //    cost the same per item; rows that cross a chunk boundary are merged by
 //    a finalize pass (tie -> earlier position, as the strict '<' scan).
@@ -29,8 +34,6 @@
 
 namespace mhb {
 namespace {
-
-constexpr unsigned kFull = 0xFFFFFFFFu;
 
 template <int SPL>
 struct Lanes {
@@ -54,11 +57,10 @@ __device__ __forceinline__ void wmh_eval(float w, float r, float c, float b, uin
   const float t = floorf(__fadd_rn(__fdiv_rn(w, r), b));
   const float tb = __fsub_rn(t, b);
   const float ln_a = __fsub_rn(__fmaf_rn(-tb, r, c), r);
-  if (ln_a < mn) {
-    mn = ln_a;
-    kk = d;
-    tf = t;
-  }
+  const bool lt = ln_a < mn;
+  mn = lt ? ln_a : mn;
+  kk = lt ? d : kk;
+  tf = lt ? t : tf;
 }
 
 __device__ __forceinline__ uint2 final_pair(uint32_t k, float t) {
@@ -129,21 +131,153 @@ __device__ __forceinline__ void store_partial(const HashArgs &a, uint32_t slot, 
   }
 }
 
+// ---- TMA bulk staging of the CSR (per warp, double-buffered) -------------
+
+constexpr uint32_t kWin = 256;  // CSR positions per staged window
+constexpr uint32_t kSpinLimit = 1u << 22;
+
+// One warp's staging area: two windows of weights (turned into ln w in
+// place) and column indices, each with its own transaction barrier.
+struct alignas(16) WarpStage {
+  float w[2][kWin];
+  uint32_t c[2][kWin];
+  unsigned long long bar[2];
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(unsigned long long *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Global -> this CTA's shared memory, completion counted on `bar`.  Both
+// addresses 16-byte aligned, bytes a multiple of 16.  No multicast.
+__device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, uint32_t bytes,
+                                              unsigned long long *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+
+// Lane 0 starts the copy of positions [ws, ws + n) into buffer `b`: the
+// 16-byte-aligned body by two bulk copies, the ragged tail is left to
+// finish_window's plain loads.
+__device__ __forceinline__ void issue_window(const HashArgs &a, WarpStage &st, uint32_t b,
+                                             uint32_t ws, uint32_t n, bool bulk_ok,
+                                             uint32_t lane) {
+  // Order this warp's earlier generic accesses of the buffer before the
+  // asynchronous writes that are about to land in it.
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  __syncwarp();
+  if (lane == 0) {
+    const uint32_t nb = bulk_ok ? (n & ~3u) : 0u;
+    if (nb) {
+      mbar_arrive_expect_tx(&st.bar[b], 8u * nb);
+      bulk_copy_g2s(st.w[b], a.weights + ws, 4u * nb, &st.bar[b]);
+      bulk_copy_g2s(st.c[b], a.cols + ws, 4u * nb, &st.bar[b]);
+    } else {
+      mbar_arrive(&st.bar[b]);
+    }
+  }
+}
+
+// Waits for buffer `b` (bounded), loads the tail, and turns weights into
+// ln(weight) in place -- once per nnz, lane-parallel.  Returns false if the
+// copy did not complete within the spin limit.
+__device__ __forceinline__ bool finish_window(const HashArgs &a, WarpStage &st, uint32_t b,
+                                              uint32_t parity, uint32_t ws, uint32_t n,
+                                              bool bulk_ok, uint32_t lane) {
+  uint32_t spins = 0;
+  while (!mbar_try_wait(&st.bar[b], parity)) {
+    if (++spins > kSpinLimit) return false;
+  }
+  const uint32_t nb = bulk_ok ? (n & ~3u) : 0u;
+  for (uint32_t i = lane; i < n; i += 32) {
+    float x;
+    if (i < nb) {
+      x = st.w[b][i];
+    } else {
+      x = __ldg(a.weights + ws + i);
+      st.c[b][i] = __ldg(a.cols + ws + i);
+    }
+    st.w[b][i] = logf(x);
+  }
+  __syncwarp();
+  return true;
+}
+
 template <int SPL>
-__global__ void __launch_bounds__(kHashBlock, 3) hash_kernel(const HashArgs a) {
+struct Params {
+  Lanes<SPL> r, c, b;
+  __device__ __forceinline__ void load(const float *__restrict__ col_base, uint32_t s_pad) {
+    r.load(col_base);
+    c.load(col_base + s_pad);
+    b.load(col_base + 2 * s_pad);
+  }
+};
+
+template <int SPL>
+__device__ __forceinline__ void eval_all(const Params<SPL> &p, float w, uint32_t d,
+                                         RowState<SPL> &st) {
+#pragma unroll
+  for (int j = 0; j < SPL; ++j) wmh_eval(w, p.r.v[j], p.c.v[j], p.b.v[j], d, st.mn[j], st.kk[j], st.tf[j]);
+}
+
+template <int SPL>
+__global__ void __launch_bounds__(kHashBlock, 4) hash_kernel(const HashArgs a) {
+  __shared__ WarpStage stage_all[kHashBlock / 32];
   if (*a.status & kStatusBadIndptr) return;
   const uint32_t lane = threadIdx.x & 31u;
+  WarpStage &stg = stage_all[threadIdx.x >> 5];
+  if (lane == 0) {
+    mbar_init(&stg.bar[0], 1);
+    mbar_init(&stg.bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncwarp();
+  uint32_t parity = 0;  // bit b: phase parity to wait for on buffer b
+
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
   const uint32_t base = a.indptr[0];
   const uint32_t items = a.nchunks * a.ntiles;
   const size_t col_stride = static_cast<size_t>(3) * a.s_pad;
+  const bool bulk_ok = ((reinterpret_cast<uintptr_t>(a.weights) |
+                         reinterpret_cast<uintptr_t>(a.cols)) & 15u) == 0;
 
   for (uint32_t item = gw; item < items; item += nw) {
     const uint32_t c = item / a.ntiles;
     const uint32_t tile = item - c * a.ntiles;
     const uint32_t s0 = tile * (32u * SPL) + lane * SPL;
     const bool active = s0 < a.s_pad;
+    const float *__restrict__ pbase = a.params + s0;
     const uint32_t cs = c * a.chunk;
     const uint32_t ce = min(a.nnz, cs + a.chunk);
     uint32_t r_next = a.chunk_row[c];
@@ -175,82 +309,83 @@ __global__ void __launch_bounds__(kHashBlock, 3) hash_kernel(const HashArgs a) {
       }
     };
 
-    // CSR block registers: lane l holds position blk + l.
-    uint32_t blk = cs;
-    float lw_cur;
-    uint32_t col_cur;
-    {
-      const uint32_t p = blk + lane;
-      const float wr = p < ce ? __ldg(a.weights + p) : 1.0f;
-      col_cur = p < ce ? __ldg(a.cols + p) : 0u;
-      lw_cur = logf(wr);
-    }
-    float w_nx = 1.0f;
-    uint32_t col_nx = 0u;
-    {
-      const uint32_t p = blk + 32u + lane;
-      if (p < ce) {
-        w_nx = __ldg(a.weights + p);
-        col_nx = __ldg(a.cols + p);
-      }
-    }
+    const uint32_t nwin = (ce - cs + kWin - 1) / kWin;
+    if (nwin > 0) issue_window(a, stg, 0, cs, min(kWin, ce - cs), bulk_ok, lane);
+    if (nwin > 1) issue_window(a, stg, 1, cs + kWin, min(kWin, ce - cs - kWin), bulk_ok, lane);
 
-    Lanes<SPL> r_c, c_c, b_c;
-    uint32_t d_cur = __shfl_sync(kFull, col_cur, 0);
-    if (cs < ce && active && d_cur < a.dim) {
-      const float *pp = a.params + d_cur * col_stride + s0;
-      r_c.load(pp);
-      c_c.load(pp + a.s_pad);
-      b_c.load(pp + 2 * a.s_pad);
-    }
+    // Error exits wait (bounded) for the windows still in flight into this
+    // warp's staging buffers before leaving: windows [from, min(from+2, nwin)).
+    auto drain = [&](uint32_t from) {
+      for (uint32_t kk = from; kk < nwin && kk < from + 2; ++kk) {
+        const uint32_t bb = kk & 1u;
+        for (uint32_t spins = 0; !mbar_try_wait(&stg.bar[bb], (parity >> bb) & 1u);)
+          if (++spins > kSpinLimit) break;
+        parity ^= 1u << bb;
+      }
+    };
 
-    for (uint32_t p = cs; p < ce; ++p) {
-      while (p >= row_end) {
-        flush();
-        // Owned rows start where the previous one ended; empty ones are
-        // flushed here with no selection.
-        if (r_next >= r_stop) {  // only reachable with inconsistent offsets
-          if (lane == 0) atomicOr(a.status, kStatusBadIndptr);
-          return;
+    for (uint32_t k = 0; k < nwin; ++k) {
+      const uint32_t b = k & 1u;
+      const uint32_t ws = cs + k * kWin;
+      const uint32_t n = min(kWin, ce - ws);
+      if (!finish_window(a, stg, b, (parity >> b) & 1u, ws, n, bulk_ok, lane)) {
+        if (lane == 0) atomicOr(a.status, kStatusStall);
+        drain(k);
+        return;
+      }
+      parity ^= 1u << b;
+      const float *__restrict__ lw = stg.w[b];
+      const uint32_t *__restrict__ cl = stg.c[b];
+
+      Params<SPL> A, B;
+      uint32_t dA = cl[0], dB = 0;
+      if (active && dA < a.dim) A.load(pbase + dA * col_stride, a.s_pad);
+      uint32_t i = 0;
+      while (i < n) {
+        // Row boundaries (warp-uniform): finish rows, start the next owned one.
+        while (ws + i >= row_end) {
+          flush();
+          if (r_next >= r_stop) {  // only reachable with inconsistent offsets
+            if (lane == 0) atomicOr(a.status, kStatusBadIndptr);
+            drain(k + 1);
+            return;
+          }
+          row = r_next++;
+          row_end = a.indptr[row + 1] - base;
+          head = false;
+          st.reset();
         }
-        row = r_next++;
-        row_end = a.indptr[row + 1] - base;
-        head = false;
-        st.reset();
-      }
-      const uint32_t pn = p + 1;
-      const uint32_t ln = pn & 31u;
-      const uint32_t d_nx = __shfl_sync(kFull, ln ? col_cur : col_nx, ln);
-      Lanes<SPL> r_n, c_n, b_n;
-      if (pn < ce && active && d_nx < a.dim) {
-        const float *pp = a.params + d_nx * col_stride + s0;
-        r_n.load(pp);
-        c_n.load(pp + a.s_pad);
-        b_n.load(pp + 2 * a.s_pad);
-      }
-      const float w = __shfl_sync(kFull, lw_cur, p & 31u);
-      if (d_cur < a.dim) {
-#pragma unroll
-        for (int j = 0; j < SPL; ++j)
-          wmh_eval(w, r_c.v[j], c_c.v[j], b_c.v[j], d_cur, st.mn[j], st.kk[j], st.tf[j]);
-      } else if (lane == 0) {
-        atomicOr(a.status, kStatusBadColumn);
-      }
-      r_c = r_n;
-      c_c = c_n;
-      b_c = b_n;
-      d_cur = d_nx;
-      if (ln == 0 && pn < ce) {
-        blk += 32u;
-        lw_cur = logf(w_nx);
-        col_cur = col_nx;
-        const uint32_t q = blk + 32u + lane;
-        w_nx = 1.0f;
-        col_nx = 0u;
-        if (q < ce) {
-          w_nx = __ldg(a.weights + q);
-          col_nx = __ldg(a.cols + q);
+        const uint32_t seg = min(row_end - ws, n);
+        // Pairs: A holds position i, B is loaded for i+1 while A is
+        // evaluated, A for i+2 while B is evaluated.
+        while (i + 1 < seg) {
+          dB = cl[i + 1];
+          if (active && dB < a.dim) B.load(pbase + dB * col_stride, a.s_pad);
+          if (dA < a.dim) eval_all<SPL>(A, lw[i], dA, st);
+          else if (lane == 0) atomicOr(a.status, kStatusBadColumn);
+          if (i + 2 < n) {
+            dA = cl[i + 2];
+            if (active && dA < a.dim) A.load(pbase + dA * col_stride, a.s_pad);
+          }
+          if (dB < a.dim) eval_all<SPL>(B, lw[i + 1], dB, st);
+          else if (lane == 0) atomicOr(a.status, kStatusBadColumn);
+          i += 2;
         }
+        if (i < seg) {
+          if (i + 1 < n) {
+            dB = cl[i + 1];
+            if (active && dB < a.dim) B.load(pbase + dB * col_stride, a.s_pad);
+          }
+          if (dA < a.dim) eval_all<SPL>(A, lw[i], dA, st);
+          else if (lane == 0) atomicOr(a.status, kStatusBadColumn);
+          ++i;
+          A = B;
+          dA = dB;
+        }
+      }
+      if (k + 2 < nwin) {
+        const uint32_t ws2 = ws + 2 * kWin;
+        issue_window(a, stg, b, ws2, min(kWin, ce - ws2), bulk_ok, lane);
       }
     }
     flush();

@@ -14,6 +14,7 @@ constexpr uint32_t kNone = 0xFFFFFFFFu;
 // Device status word bits (written by kernels, read by the host).
 constexpr uint32_t kStatusBadColumn = 1u;  // a column index >= dim was seen
 constexpr uint32_t kStatusBadIndptr = 2u;  // row offsets decrease or disagree with nnz
+constexpr uint32_t kStatusStall = 4u;      // a bounded wait on a staging copy gave up
 
 // Parameter table: one contiguous block per column d,
 //   params[(d * 3 + 0) * s_pad + s] = r      (rs)
