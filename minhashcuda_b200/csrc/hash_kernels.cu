@@ -279,7 +279,7 @@ __global__ void __launch_bounds__(kHashBlock, 4) hash_kernel(const HashArgs a) {
     const bool active = s0 < a.s_pad;
     const float *__restrict__ pbase = a.params + s0;
     const uint32_t cs = c * a.chunk;
-    const uint32_t ce = min(a.nnz, cs + a.chunk);
+    const uint32_t ce = cs + min(a.chunk, a.nnz - cs);  // no uint32 overflow near 2^32
     uint32_t r_next = a.chunk_row[c];
     const uint32_t r_stop = (c + 1 < a.nchunks) ? a.chunk_row[c + 1] : a.rows;
 
@@ -414,7 +414,7 @@ __global__ void finalize_kernel(const HashArgs a) {
     if (r1 <= r0) continue;
     const uint32_t row = r1 - 1;
     const uint32_t end = a.indptr[row + 1] - base;
-    const uint32_t ce = min(a.nnz, c * a.chunk + a.chunk);
+    const uint32_t ce = c * a.chunk + min(a.chunk, a.nnz - c * a.chunk);
     if (end <= ce) continue;
     const uint32_t c_last = (end - 1) / a.chunk;
     uint32_t *o = a.out + static_cast<size_t>(row) * a.samples * 2;
