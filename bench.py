@@ -301,8 +301,14 @@ def main():
     alg_bytes = 12 * nnz * S + 8 * nnz + 4 * (R + 1) + 8 * R * S
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (hash_ms_launch / 1e3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "hash_kernel_traffic.json")
+    if os.path.exists(tp) and w.name == "large":
+        traffic = json.load(open(tp))["dram_bytes_per_eval"] * evals
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": None, "kernel": "hash_kernel",
+                "frac": achieved / peak, "traffic": traffic, "kernel": "hash_kernel",
+                "traffic_source": "profiles/hash_kernel_traffic.json (ncu, 20k-row case, "
+                                  "scaled by evals)" if traffic else None,
                 "kernel_ms": hash_ms_launch, "algorithmic_bytes": alg_bytes,
                 "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)"}
 
