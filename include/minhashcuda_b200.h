@@ -38,6 +38,34 @@ enum MHCUDAResult mhcuda_calc_device(
  * kernel.cu:166-170). */
 enum MHCUDAResult mhcuda_device_status(const MinhashCudaGenerator *gen);
 
+/* Allocation-free variant of mhcuda_calc_device, same arguments, for
+ * callers that must not allocate device memory: processes whose device
+ * memory another allocator (a framework's caching allocator, say) has
+ * already reserved, where a cudaMalloc would fail, and latency-critical
+ * loops that cannot take the device-wide synchronisation a cudaMalloc or
+ * cudaFree may cause.  mhcuda_calc_device grows a workspace with cudaMalloc;
+ * this call instead uses one fixed 8 MiB array of device memory that is part
+ * of the library (every GPU that loads the library holds it until the process
+ * exits) and calls no allocating routine.
+ *  - Limit: an input needs 4 + 24*s_pad bytes per chunk of at most 2^20 nnz
+ *    (s_pad = samples rounded up to a multiple of 4); it is refused with
+ *    mhcudaInvalidArguments when ceil(nnz / 2^20) chunks do not fit in
+ *    8 MiB - 1 KiB (about 2.8e9 nnz at 128 samples, 5*2^20 at 65535).
+ *  - The first call on a device looks up the array's device address and
+ *    caches it; make that first call before any stream capture begins.
+ *  - All calls share the array, which keeps the last call's contents: the
+ *    status word is cleared by every call and everything else a call reads it
+ *    writes first.  Calls whose work overlapped on the GPU would race on the
+ *    array, so every call waits for its own work to finish before it returns
+ *    and calls are serialised by a process-wide lock.
+ *  - Returns mhcudaInvalidArguments for invalid CSR content (a column >= dim,
+ *    decreasing offsets) as detected on the device.
+ * No counterpart in the reference. */
+enum MHCUDAResult mhcuda_calc_device_noalloc(
+    const MinhashCudaGenerator *gen, const float *d_weights,
+    const uint32_t *d_cols, const uint32_t *d_rows, uint32_t length,
+    uint32_t nnz, uint32_t *d_output, void *stream);
+
 /* Hashes `count` independent CSR matrices (host buffers, as in mhcuda_calc)
  * against one generator in one device pass: the matrices are staged
  * back to back, one persistent launch walks a (matrix, row-chunk) work list

@@ -325,6 +325,23 @@ MHCUDAResult init_params(Gen *gen, uint32_t seed) {
 
 }  // namespace
 
+namespace mhb {
+
+bool generator_view(const MinhashCudaGenerator_ *gen, GeneratorView *view) {
+  if (!gen || !view) return false;
+  view->params = gen->params;
+  view->dim = gen->dim;
+  view->samples = gen->samples;
+  view->s_pad = gen->s_pad;
+  view->device = gen->device;
+  view->sm_count = gen->sm_count;
+  view->verbosity = gen->verbosity;
+  view->stream = gen->stream;
+  return true;
+}
+
+}  // namespace mhb
+
 extern "C" {
 
 MinhashCudaGenerator *mhcuda_init(uint32_t dim, uint16_t samples, uint32_t seed, int deferred,

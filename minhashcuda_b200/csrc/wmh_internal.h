@@ -7,6 +7,8 @@
 
 #include <cuda_runtime.h>
 
+struct MinhashCudaGenerator_;
+
 namespace mhb {
 
 constexpr uint32_t kNone = 0xFFFFFFFFu;
@@ -85,5 +87,19 @@ cudaError_t launch_unpack_params(const float *params, uint32_t which, uint32_t d
                                  uint32_t samples, uint32_t s_pad, float *dst,
                                  cudaStream_t stream);
 cudaError_t launch_logf(const float *in, float *out, size_t n, cudaStream_t stream);
+
+// Read-only view of a generator's fields for entry points that live outside
+// engine.cu (engine.cu).
+struct GeneratorView {
+  const float *params;
+  uint32_t dim;
+  uint32_t samples;
+  uint32_t s_pad;
+  int device;
+  int sm_count;
+  int verbosity;
+  cudaStream_t stream;
+};
+bool generator_view(const MinhashCudaGenerator_ *gen, GeneratorView *view);
 
 }  // namespace mhb
