@@ -134,6 +134,18 @@ struct MinhashCudaGenerator_ {
   mutable DevBuf d_weights, d_cols, d_indptr, d_out, d_chunk_row, d_part_ln, d_part_kt, d_status;
   mutable PinnedBuf h_status;
   mutable PinnedBuf h_stage;      // batch staging (weights | cols | indptr)
+  // Row-block pipeline of mhcuda_calc: two slots, each a block's device CSR,
+  // hashes and (for pageable caller buffers) pinned staging.
+  struct Slot {
+    DevBuf w, c, ip, out;
+    PinnedBuf hw, hc, hip, hout;
+    cudaEvent_t h2d = nullptr, done = nullptr, d2h = nullptr;
+    bool busy = false;              // holds an enqueued block
+    uint32_t *pending_out = nullptr;  // caller destination of a staged block of hashes
+    size_t pending_bytes = 0;
+  };
+  mutable Slot slots[2];
+  mutable cudaStream_t s_in = nullptr, s_out = nullptr;
   // Optional timing of every hash-kernel launch with CUDA events recorded on
   // the launch stream (mhcuda_profile / mhcuda_profile_read).
   mutable bool profiling = false;
@@ -150,6 +162,15 @@ struct MinhashCudaGenerator_ {
       cudaEventDestroy(e.first);
       cudaEventDestroy(e.second);
     }
+    for (auto &sl : slots) {
+      if (sl.h2d) cudaEventDestroy(sl.h2d);
+      if (sl.done) cudaEventDestroy(sl.done);
+      if (sl.d2h) cudaEventDestroy(sl.d2h);
+      sl.w.release(); sl.c.release(); sl.ip.release(); sl.out.release();
+      sl.hw.release(); sl.hc.release(); sl.hip.release(); sl.hout.release();
+    }
+    if (s_in) cudaStreamDestroy(s_in);
+    if (s_out) cudaStreamDestroy(s_out);
     if (params) cudaFree(params);
     if (stream) cudaStreamDestroy(stream);
   }
@@ -246,8 +267,9 @@ MHCUDAResult prepare_launch(const Gen *gen, uint32_t rows, uint32_t nnz, const H
 }
 
 MHCUDAResult enqueue_hash(const Gen *gen, const HashArgs &a, const HashPlan &plan,
-                          cudaStream_t stream) {
-  MHB_CHECK(gen, cudaMemsetAsync(a.status, 0, sizeof(uint32_t), stream), mhcudaRuntimeError);
+                          cudaStream_t stream, bool clear_status = true) {
+  if (clear_status)
+    MHB_CHECK(gen, cudaMemsetAsync(a.status, 0, sizeof(uint32_t), stream), mhcudaRuntimeError);
   MHB_CHECK(gen, mhb::launch_plan(a, stream), mhcudaRuntimeError);
   std::pair<cudaEvent_t, cudaEvent_t> *ev = nullptr;
   if (gen->profiling) {
@@ -278,6 +300,167 @@ MHCUDAResult read_status(const Gen *gen, cudaStream_t stream) {
     return mhcudaInvalidArguments;
   }
   return mhcudaSuccess;
+}
+
+// True when `p` is page-locked host memory the copy engines can read directly.
+bool is_pinned(const void *p) {
+  cudaPointerAttributes attr{};
+  if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return attr.type == cudaMemoryTypeHost;
+}
+
+// memcpy split over a few threads for large blocks (host bandwidth for the
+// pinned staging of pageable caller buffers).
+void par_memcpy(void *dst, const void *src, size_t bytes) {
+  const size_t kSplit = static_cast<size_t>(8) << 20;
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const unsigned n = bytes < kSplit ? 1u : std::min<unsigned>(8u, hw);
+  if (n == 1) {
+    memcpy(dst, src, bytes);
+    return;
+  }
+  const size_t part = (((bytes + n - 1) / n) + 4095) & ~static_cast<size_t>(4095);
+  std::vector<std::thread> pool;
+  for (unsigned t = 0; t < n; ++t) {
+    const size_t off = t * part;
+    if (off >= bytes) break;
+    const size_t len = std::min(part, bytes - off);
+    pool.emplace_back([=]() {
+      memcpy(static_cast<char *>(dst) + off, static_cast<const char *>(src) + off, len);
+    });
+  }
+  for (auto &th : pool) th.join();
+}
+
+// Inputs with at least this many nnz go through the row-block pipeline.
+constexpr uint64_t kPipelineMinNnz = 16ull << 20;
+
+// mhcuda_calc for large inputs: rows are cut into blocks of about
+// `block_nnz` entries; block i's hashes run on the generator stream while
+// block i+1 is copied in on s_in and block i-1's hashes are copied out on
+// s_out.  Caller buffers that are page-locked are copied directly; pageable
+// ones go through pinned staging filled by host threads.
+MHCUDAResult calc_pipelined(const Gen *gen, const float *weights, const uint32_t *cols,
+                            const uint32_t *rows, uint32_t length, uint32_t *output) {
+  const cudaStream_t st = gen->stream;
+  if (!gen->s_in) {
+    MHB_CHECK(gen, cudaStreamCreateWithFlags(&gen->s_in, cudaStreamNonBlocking),
+              mhcudaRuntimeError);
+    MHB_CHECK(gen, cudaStreamCreateWithFlags(&gen->s_out, cudaStreamNonBlocking),
+              mhcudaRuntimeError);
+    for (auto &sl : gen->slots) {
+      MHB_CHECK(gen, cudaEventCreateWithFlags(&sl.h2d, cudaEventDisableTiming), mhcudaRuntimeError);
+      MHB_CHECK(gen, cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming), mhcudaRuntimeError);
+      MHB_CHECK(gen, cudaEventCreateWithFlags(&sl.d2h, cudaEventDisableTiming), mhcudaRuntimeError);
+    }
+  }
+  const uint64_t nnz = static_cast<uint64_t>(rows[length]) - rows[0];
+  uint64_t block_nnz = std::min<uint64_t>(std::max<uint64_t>(nnz / 8, 8ull << 20), 256ull << 20);
+  const int forced = env_int("MHCUDA_B200_BLOCK_NNZ", 0);
+  if (forced > 0) block_nnz = static_cast<uint64_t>(forced);
+  const bool pin_in = is_pinned(weights) && is_pinned(cols) && is_pinned(rows);
+  const bool pin_out = is_pinned(output);
+  const size_t row_bytes = static_cast<size_t>(gen->samples) * 2 * sizeof(uint32_t);
+  MHB_CHECK(gen, gen->d_status.ensure(sizeof(uint32_t)), mhcudaMemoryAllocationFailure);
+  MHB_CHECK(gen, cudaMemsetAsync(gen->d_status.ptr, 0, sizeof(uint32_t), st), mhcudaRuntimeError);
+
+  // Finishes a slot: waits for its hashes and moves staged ones to the caller.
+  auto retire = [&](Gen::Slot &sl) -> MHCUDAResult {
+    if (!sl.busy) return mhcudaSuccess;
+    MHB_CHECK(gen, cudaEventSynchronize(sl.d2h), mhcudaMemoryCopyError);
+    if (sl.pending_out) par_memcpy(sl.pending_out, sl.hout.ptr, sl.pending_bytes);
+    sl.pending_out = nullptr;
+    sl.busy = false;
+    return mhcudaSuccess;
+  };
+
+  MHCUDAResult r = mhcudaSuccess;
+  uint32_t r0 = 0;
+  for (uint32_t i = 0; r0 < length && r == mhcudaSuccess; ++i) {
+    // Block [r0, r1): as many rows as fit in block_nnz (at least one).
+    const uint64_t limit = static_cast<uint64_t>(rows[r0]) + block_nnz;
+    uint32_t r1 = static_cast<uint32_t>(
+        std::upper_bound(rows + r0 + 1, rows + length + 1, limit,
+                         [](uint64_t v, uint32_t x) { return v < x; }) - rows) - 1;
+    r1 = std::max(r1, r0 + 1);
+    Gen::Slot &sl = gen->slots[i & 1];
+    r = retire(sl);
+    if (r != mhcudaSuccess) break;
+    const uint32_t len = r1 - r0;
+    const uint32_t b0 = rows[r0];
+    const uint32_t n = rows[r1] - b0;
+    MHB_CHECK(gen, sl.w.ensure(static_cast<size_t>(n) * 4 + 16), mhcudaMemoryAllocationFailure);
+    MHB_CHECK(gen, sl.c.ensure(static_cast<size_t>(n) * 4 + 16), mhcudaMemoryAllocationFailure);
+    MHB_CHECK(gen, sl.ip.ensure((static_cast<size_t>(len) + 1) * 4), mhcudaMemoryAllocationFailure);
+    MHB_CHECK(gen, sl.out.ensure(len * row_bytes), mhcudaMemoryAllocationFailure);
+    const void *src_w = weights + b0, *src_c = cols + b0, *src_i = rows + r0;
+    if (!pin_in) {
+      MHB_CHECK(gen, sl.hw.ensure(static_cast<size_t>(n) * 4), mhcudaMemoryAllocationFailure);
+      MHB_CHECK(gen, sl.hc.ensure(static_cast<size_t>(n) * 4), mhcudaMemoryAllocationFailure);
+      MHB_CHECK(gen, sl.hip.ensure((static_cast<size_t>(len) + 1) * 4),
+                mhcudaMemoryAllocationFailure);
+      par_memcpy(sl.hw.ptr, src_w, static_cast<size_t>(n) * 4);
+      par_memcpy(sl.hc.ptr, src_c, static_cast<size_t>(n) * 4);
+      memcpy(sl.hip.ptr, src_i, (static_cast<size_t>(len) + 1) * 4);
+      src_w = sl.hw.ptr;
+      src_c = sl.hc.ptr;
+      src_i = sl.hip.ptr;
+    }
+    MHB_CHECK(gen, cudaMemcpyAsync(sl.ip.ptr, src_i, (static_cast<size_t>(len) + 1) * 4,
+                                   cudaMemcpyHostToDevice, gen->s_in),
+              mhcudaMemoryCopyError);
+    if (n) {
+      MHB_CHECK(gen, cudaMemcpyAsync(sl.w.ptr, src_w, static_cast<size_t>(n) * 4,
+                                     cudaMemcpyHostToDevice, gen->s_in),
+                mhcudaMemoryCopyError);
+      MHB_CHECK(gen, cudaMemcpyAsync(sl.c.ptr, src_c, static_cast<size_t>(n) * 4,
+                                     cudaMemcpyHostToDevice, gen->s_in),
+                mhcudaMemoryCopyError);
+    }
+    MHB_CHECK(gen, cudaEventRecord(sl.h2d, gen->s_in), mhcudaRuntimeError);
+    MHB_CHECK(gen, cudaStreamWaitEvent(st, sl.h2d, 0), mhcudaRuntimeError);
+    const HashPlan plan = make_plan(gen, n, len);
+    HashArgs a{};
+    r = prepare_launch(gen, len, n, plan, &a);
+    if (r != mhcudaSuccess) break;
+    a.weights = sl.w.as<float>();
+    a.cols = sl.c.as<uint32_t>();
+    a.indptr = sl.ip.as<uint32_t>();
+    a.out = sl.out.as<uint32_t>();
+    r = enqueue_hash(gen, a, plan, st, /*clear_status=*/false);
+    if (r != mhcudaSuccess) break;
+    MHB_CHECK(gen, cudaEventRecord(sl.done, st), mhcudaRuntimeError);
+    MHB_CHECK(gen, cudaStreamWaitEvent(gen->s_out, sl.done, 0), mhcudaRuntimeError);
+    uint32_t *dst = output + static_cast<size_t>(r0) * gen->samples * 2;
+    if (pin_out) {
+      MHB_CHECK(gen, cudaMemcpyAsync(dst, sl.out.ptr, len * row_bytes, cudaMemcpyDeviceToHost,
+                                     gen->s_out),
+                mhcudaMemoryCopyError);
+    } else {
+      MHB_CHECK(gen, sl.hout.ensure(len * row_bytes), mhcudaMemoryAllocationFailure);
+      MHB_CHECK(gen, cudaMemcpyAsync(sl.hout.ptr, sl.out.ptr, len * row_bytes,
+                                     cudaMemcpyDeviceToHost, gen->s_out),
+                mhcudaMemoryCopyError);
+      sl.pending_out = dst;
+      sl.pending_bytes = len * row_bytes;
+    }
+    MHB_CHECK(gen, cudaEventRecord(sl.d2h, gen->s_out), mhcudaRuntimeError);
+    sl.busy = true;
+    MHB_DEBUG(gen, "block %u: rows [%u, %u) nnz %u chunk %u\n", i, r0, r1, n, plan.chunk);
+    r0 = r1;
+  }
+  for (auto &sl : gen->slots) {
+    const MHCUDAResult rr = retire(sl);
+    if (r == mhcudaSuccess) r = rr;
+  }
+  if (r != mhcudaSuccess) {
+    cudaDeviceSynchronize();
+    return r;
+  }
+  return read_status(gen, st);
 }
 
 MHCUDAResult init_params(Gen *gen, uint32_t seed) {
@@ -471,6 +654,10 @@ enum MHCUDAResult mhcuda_calc(const MinhashCudaGenerator *gen, const float *weig
   if (rows[length] < base) return mhcudaInvalidArguments;
   const uint32_t nnz = rows[length] - base;
   const cudaStream_t st = gen->stream;
+  const int min_override = env_int("MHCUDA_B200_PIPELINE_MIN_NNZ", 0);
+  const uint64_t pipe_min = min_override > 0 ? static_cast<uint64_t>(min_override) : kPipelineMinNnz;
+  if (nnz >= pipe_min && env_int("MHCUDA_B200_NO_PIPELINE", 0) == 0)
+    return calc_pipelined(gen, weights, cols, rows, length, output);
   MHB_CHECK(gen, gen->d_weights.ensure(static_cast<size_t>(nnz) * 4 + 16),
             mhcudaMemoryAllocationFailure);
   MHB_CHECK(gen, gen->d_cols.ensure(static_cast<size_t>(nnz) * 4 + 16),

@@ -171,3 +171,63 @@ def test_batch_equals_plain_calls():
     for b, p in zip(batch, plain):
         np.testing.assert_array_equal(b, p)
     del minhashcuda_b200
+
+
+def _pinned(a):
+    """A copy of numpy array `a` in page-locked host memory."""
+    import torch
+    t = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True)
+    v = t.numpy().view(a.dtype)[:a.size].reshape(a.shape)
+    v[...] = a
+    return v, t
+
+
+@pytest.mark.parametrize("pinned", [False, True])
+@pytest.mark.parametrize("block_nnz", [1000, 7777, 100000])
+def test_row_block_pipeline(monkeypatch, pinned, block_nnz):
+    """mhcuda_calc's H2D/compute/D2H pipeline over row blocks equals the
+    single-launch path and the oracle, for pageable and page-locked buffers
+    and blocks smaller than a row."""
+    rng = np.random.default_rng(block_nnz + int(pinned))
+    dim = 6000
+    params = gamma_params(rng, dim, 128)
+    m = random_csr(rng, 900, dim, 120, long_rows=[(3, 5000), (450, 2500)], empty_frac=0.02)
+    want = O.COracle(*params).hash_csr(m, lnw=device_logf(m.data))
+    with engine_gen(dim, 128, deferred=True) as eng:
+        eng.assign(*params)
+        monkeypatch.setenv("MHCUDA_B200_PIPELINE_MIN_NNZ", "1")
+        monkeypatch.setenv("MHCUDA_B200_BLOCK_NNZ", str(block_nnz))
+        data, idx, ip = m.data, m.indices.astype(np.uint32), m.indptr.astype(np.uint32)
+        keep = []
+        out = np.full((m.shape[0], 128, 2), 7, np.uint32)
+        if pinned:
+            (data, t1), (idx, t2), (ip, t3), (out, t4) = (_pinned(data), _pinned(idx), _pinned(ip),
+                                                          _pinned(out))
+            keep = [t1, t2, t3, t4]
+        rc = eng.lib.mhcuda_calc(eng.h, data.ctypes.data, idx.ctypes.data, ip.ctypes.data,
+                                 m.shape[0], out.ctypes.data)
+        assert rc == 0
+        np.testing.assert_array_equal(out, want)
+        # twice in a row (slot reuse), then the single-launch path
+        rc = eng.lib.mhcuda_calc(eng.h, data.ctypes.data, idx.ctypes.data, ip.ctypes.data,
+                                 m.shape[0], out.ctypes.data)
+        assert rc == 0
+        np.testing.assert_array_equal(out, want)
+        monkeypatch.setenv("MHCUDA_B200_NO_PIPELINE", "1")
+        np.testing.assert_array_equal(eng.calc_csr(m), want)
+        del keep
+
+
+def test_row_block_pipeline_reports_bad_column_in_late_block(monkeypatch):
+    rng = np.random.default_rng(77)
+    dim = 500
+    m = random_csr(rng, 400, dim, 30)
+    idx = m.indices.astype(np.uint32).copy()
+    idx[-3] = dim + 5
+    with engine_gen(dim, 64, seed=3) as eng:
+        monkeypatch.setenv("MHCUDA_B200_PIPELINE_MIN_NNZ", "1")
+        monkeypatch.setenv("MHCUDA_B200_BLOCK_NNZ", "1000")
+        rc, _ = eng.calc_raw(m.data, idx, m.indptr)
+        assert rc == 1
+        out = eng.calc_csr(m)  # still usable
+        assert out.shape == (400, 64, 2)
