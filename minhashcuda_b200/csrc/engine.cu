@@ -214,9 +214,14 @@ HashPlan make_plan(const Gen *gen, uint64_t nnz, uint64_t rows) {
     if (evals < (1ull << 26) && spl > 1) spl = 1;  // small inputs: more items
   }
   p.spl = static_cast<uint32_t>(spl);
+  p.minb = 4;
+  if (p.spl == 4) {
+    const int minb = env_int("MHCUDA_B200_MINB", 4);
+    p.minb = minb == 3 ? 3u : 4u;
+  }
   const uint32_t tile_w = 32u * p.spl;
   p.ntiles = (s_pad + tile_w - 1) / tile_w;
-  const int bps = mhb::hash_blocks_per_sm(p.spl);
+  const int bps = mhb::hash_blocks_per_sm(p.spl, p.minb);
   const uint64_t resident_warps =
       static_cast<uint64_t>(gen->sm_count) * bps * (mhb::kHashBlock / 32);
   const int waves = std::max(1, env_int("MHCUDA_B200_WAVES", 32));

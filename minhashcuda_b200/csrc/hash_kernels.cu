@@ -51,10 +51,38 @@ struct Lanes {
   }
 };
 
-// One (nnz, sample) evaluation, kernel.cu:101-109.
-__device__ __forceinline__ void wmh_eval(float w, float r, float c, float b, uint32_t d,
-                                         float &mn, uint32_t &kk, float &tf) {
-  const float t = floorf(__fadd_rn(__fdiv_rn(w, r), b));
+// t of kernel.cu:103 exactly as the reference computes it: IEEE quotient,
+// rounded sum, floor.
+__device__ __forceinline__ float exact_t(float w, float r, float b) {
+  return floorf(__fadd_rn(__fdiv_rn(w, r), b));
+}
+
+// Margin of the fast t below, relative to |w/r| + |beta| + 1.
+constexpr float kTMargin = 0x1p-18f;
+
+// Fast t.  Only floor(v) with v = RN(RN(w/r) + beta) is needed, and it only
+// depends on the exact quotient when v lies close to an integer.  With
+// y = rcp.approx(r) (documented error 1 ulp; 2^-22 relative assumed) and
+// va = RN(RN(w*y) + beta):
+//   |va - v| <= |w/r| * 2^-20.6 + |beta| * 2^-23 < m,
+//   m = (|w*y| + |beta| + 1) * 2^-18,
+// so when va is more than m away from every integer, floor(va) = floor(v).
+// Returns false (t undecided) otherwise, and for every non-finite or
+// flushed case (w = +-inf/NaN, r = 0/denormal/huge, |va| >= 2^22: m >= 16).
+__device__ __forceinline__ bool fast_t(float w, float r, float b, float &t) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(r));
+  const float qa = __fmul_rn(w, y);
+  const float va = __fadd_rn(qa, b);
+  t = floorf(va);
+  const float f = __fsub_rn(va, t);  // exact for |va| >= 1; 1.0 or exact for va in (-1, 1)
+  const float m = __fmaf_rn(__fadd_rn(fabsf(qa), fabsf(b)), kTMargin, kTMargin);
+  return fabsf(__fsub_rn(f, 0.5f)) < __fsub_rn(0.5f, m);  // NaN -> false
+}
+
+// One (nnz, sample) evaluation, kernel.cu:101-109, given t.
+__device__ __forceinline__ void wmh_update(float t, float r, float c, float b, uint32_t d,
+                                           float &mn, uint32_t &kk, float &tf) {
   const float tb = __fsub_rn(t, b);
   const float ln_a = __fsub_rn(__fmaf_rn(-tb, r, c), r);
   const bool lt = ln_a < mn;
@@ -244,14 +272,25 @@ struct Params {
 };
 
 template <int SPL>
-__device__ __forceinline__ void eval_all(const Params<SPL> &p, float w, uint32_t d,
+__device__ __forceinline__ void eval_all(const Params<SPL> &p, float w, uint32_t d, bool active,
                                          RowState<SPL> &st) {
+  float t[SPL];
+  bool undecided = false;
 #pragma unroll
-  for (int j = 0; j < SPL; ++j) wmh_eval(w, p.r.v[j], p.c.v[j], p.b.v[j], d, st.mn[j], st.kk[j], st.tf[j]);
+  for (int j = 0; j < SPL; ++j) undecided |= !fast_t(w, p.r.v[j], p.b.v[j], t[j]);
+  // Rare: some lane's t sits within the margin of an integer; the warp takes
+  // the exact quotient for all its samples (warp-uniform branch).
+  if (__any_sync(0xFFFFFFFFu, undecided && active)) {
+#pragma unroll
+    for (int j = 0; j < SPL; ++j) t[j] = exact_t(w, p.r.v[j], p.b.v[j]);
+  }
+#pragma unroll
+  for (int j = 0; j < SPL; ++j)
+    wmh_update(t[j], p.r.v[j], p.c.v[j], p.b.v[j], d, st.mn[j], st.kk[j], st.tf[j]);
 }
 
-template <int SPL>
-__global__ void __launch_bounds__(kHashBlock, 4) hash_kernel(const HashArgs a) {
+template <int SPL, int MINB>
+__global__ void __launch_bounds__(kHashBlock, MINB) hash_kernel(const HashArgs a) {
   __shared__ WarpStage stage_all[kHashBlock / 32];
   if (*a.status & kStatusBadIndptr) return;
   const uint32_t lane = threadIdx.x & 31u;
@@ -361,13 +400,13 @@ __global__ void __launch_bounds__(kHashBlock, 4) hash_kernel(const HashArgs a) {
         while (i + 1 < seg) {
           dB = cl[i + 1];
           if (active && dB < a.dim) B.load(pbase + dB * col_stride, a.s_pad);
-          if (dA < a.dim) eval_all<SPL>(A, lw[i], dA, st);
+          if (dA < a.dim) eval_all<SPL>(A, lw[i], dA, active, st);
           else if (lane == 0) atomicOr(a.status, kStatusBadColumn);
           if (i + 2 < n) {
             dA = cl[i + 2];
             if (active && dA < a.dim) A.load(pbase + dA * col_stride, a.s_pad);
           }
-          if (dB < a.dim) eval_all<SPL>(B, lw[i + 1], dB, st);
+          if (dB < a.dim) eval_all<SPL>(B, lw[i + 1], dB, active, st);
           else if (lane == 0) atomicOr(a.status, kStatusBadColumn);
           i += 2;
         }
@@ -376,7 +415,7 @@ __global__ void __launch_bounds__(kHashBlock, 4) hash_kernel(const HashArgs a) {
             dB = cl[i + 1];
             if (active && dB < a.dim) B.load(pbase + dB * col_stride, a.s_pad);
           }
-          if (dA < a.dim) eval_all<SPL>(A, lw[i], dA, st);
+          if (dA < a.dim) eval_all<SPL>(A, lw[i], dA, active, st);
           else if (lane == 0) atomicOr(a.status, kStatusBadColumn);
           ++i;
           A = B;
@@ -450,13 +489,27 @@ cudaError_t launch_plan(const HashArgs &a, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_hash(const HashArgs &a, const HashPlan &plan, cudaStream_t stream) {
-  switch (plan.spl) {
-    case 4: hash_kernel<4><<<plan.grid, kHashBlock, 0, stream>>>(a); break;
-    case 2: hash_kernel<2><<<plan.grid, kHashBlock, 0, stream>>>(a); break;
-    case 1: hash_kernel<1><<<plan.grid, kHashBlock, 0, stream>>>(a); break;
-    default: return cudaErrorInvalidValue;
+namespace {
+
+using HashFn = void (*)(const HashArgs);
+
+// Instantiated (samples per lane, minimum resident blocks per SM) variants.
+HashFn pick_hash(uint32_t spl, uint32_t minb) {
+  switch (spl * 10 + minb) {
+    case 44: return hash_kernel<4, 4>;
+    case 43: return hash_kernel<4, 3>;
+    case 24: return hash_kernel<2, 4>;
+    case 14: return hash_kernel<1, 4>;
+    default: return nullptr;
   }
+}
+
+}  // namespace
+
+cudaError_t launch_hash(const HashArgs &a, const HashPlan &plan, cudaStream_t stream) {
+  const HashFn fn = pick_hash(plan.spl, plan.minb);
+  if (!fn) return cudaErrorInvalidValue;
+  fn<<<plan.grid, kHashBlock, 0, stream>>>(a);
   return cudaGetLastError();
 }
 
@@ -468,26 +521,20 @@ cudaError_t launch_finalize(const HashArgs &a, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
-int hash_blocks_per_sm(uint32_t spl) {
+int hash_blocks_per_sm(uint32_t spl, uint32_t minb) {
+  const HashFn fn = pick_hash(spl, minb);
   int n = 0;
-  cudaError_t e = cudaErrorInvalidValue;
-  switch (spl) {
-    case 4: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, hash_kernel<4>, kHashBlock, 0); break;
-    case 2: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, hash_kernel<2>, kHashBlock, 0); break;
-    case 1: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, hash_kernel<1>, kHashBlock, 0); break;
-    default: break;
+  if (!fn || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kHashBlock, 0) != cudaSuccess) {
+    cudaGetLastError();
+    return 1;
   }
-  return e == cudaSuccess && n > 0 ? n : 1;
+  return n > 0 ? n : 1;
 }
 
-size_t hash_kernel_registers(uint32_t spl) {
+size_t hash_kernel_registers(uint32_t spl, uint32_t minb) {
+  const HashFn fn = pick_hash(spl, minb);
   cudaFuncAttributes attr{};
-  switch (spl) {
-    case 4: cudaFuncGetAttributes(&attr, hash_kernel<4>); break;
-    case 2: cudaFuncGetAttributes(&attr, hash_kernel<2>); break;
-    case 1: cudaFuncGetAttributes(&attr, hash_kernel<1>); break;
-    default: break;
-  }
+  if (!fn || cudaFuncGetAttributes(&attr, fn) != cudaSuccess) return 0;
   return attr.numRegs;
 }
 

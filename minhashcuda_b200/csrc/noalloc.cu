@@ -86,6 +86,7 @@ extern "C" enum MHCUDAResult mhcuda_calc_device_noalloc(
   };
   mhb::HashPlan plan{};
   plan.spl = util(4) >= 0.75 ? 4 : (util(2) >= 0.75 ? 2 : 1);
+  plan.minb = 4;
   plan.ntiles = (s_pad + 32u * plan.spl - 1) / (32u * plan.spl);
   const uint64_t per_chunk = 4 + 2 * static_cast<uint64_t>(s_pad) * (sizeof(float) + sizeof(uint2));
   const uint64_t max_chunks = (kNoallocScratchBytes - 1024) / per_chunk;
@@ -115,7 +116,7 @@ extern "C" enum MHCUDAResult mhcuda_calc_device_noalloc(
   char *scratch = static_cast<char *>(noalloc_scratch_on(g.device));
   if (!scratch) return mhcudaRuntimeError;
   const cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : g.stream;
-  const int bps = mhb::hash_blocks_per_sm(plan.spl);
+  const int bps = mhb::hash_blocks_per_sm(plan.spl, plan.minb);
   const uint64_t items = static_cast<uint64_t>(plan.nchunks) * plan.ntiles;
   const uint64_t want = (items + mhb::kHashBlock / 32 - 1) / (mhb::kHashBlock / 32);
   plan.grid = static_cast<uint32_t>(

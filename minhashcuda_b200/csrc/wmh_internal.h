@@ -41,6 +41,7 @@ struct HashPlan {
   uint32_t chunk;    // positions per chunk, multiple of 32
   uint32_t nchunks;  // >= 1
   uint32_t spl;      // samples per lane in one item: 1, 2 or 4
+  uint32_t minb;     // kernel variant: minimum resident blocks per SM (4, or 3 for spl 4)
   uint32_t ntiles;   // sample tiles of 32*spl samples
   uint32_t grid;     // persistent grid (blocks of kHashBlock threads)
 };
@@ -73,8 +74,8 @@ cudaError_t launch_plan(const HashArgs &a, cudaStream_t stream);
 cudaError_t launch_hash(const HashArgs &a, const HashPlan &plan, cudaStream_t stream);
 cudaError_t launch_finalize(const HashArgs &a, cudaStream_t stream);
 // Blocks per SM the hash kernel reaches for a given samples-per-lane value.
-int hash_blocks_per_sm(uint32_t spl);
-size_t hash_kernel_registers(uint32_t spl);
+int hash_blocks_per_sm(uint32_t spl, uint32_t minb);
+size_t hash_kernel_registers(uint32_t spl, uint32_t minb);
 
 // Parameter kernels (param_kernels.cu).
 enum class PairOp : int { kGamma = 0, kLogGamma = 1, kCopy = 2 };

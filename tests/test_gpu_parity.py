@@ -231,3 +231,23 @@ def test_row_block_pipeline_reports_bad_column_in_late_block(monkeypatch):
         assert rc == 1
         out = eng.calc_csr(m)  # still usable
         assert out.shape == (400, 64, 2)
+
+
+def test_near_integer_quotients():
+    """w/r + beta within 1e-9..1e-3 of an integer on either side: the fast
+    reciprocal path must hand every such case to the exact IEEE quotient."""
+    rng = np.random.default_rng(21)
+    dim, samples = 3000, 128
+    wt = np.exp(rng.uniform(-6, 6, dim)).astype(np.float32)
+    w = np.log(wt.astype(np.float64))
+    rs = rng.uniform(0.02, 6.0, (samples, dim))
+    q = w[None, :] / rs
+    delta = rng.choice([-1.0, 1.0], (samples, dim)) * 10.0 ** rng.uniform(-9, -3, (samples, dim))
+    b = np.round(q) - q + delta
+    lc = np.log(rng.gamma(2.0, 1.0, (samples, dim)))
+    params = (rs.astype(np.float32), lc.astype(np.float32), b.astype(np.float32))
+    # one row per column (the crafted weight alone), then rows mixing columns
+    single = sp.csr_matrix((wt, np.arange(dim), np.arange(dim + 1)), shape=(dim, dim))
+    mixed = random_csr(rng, 500, dim, 40)
+    mixed = sp.csr_matrix((wt[mixed.indices], mixed.indices, mixed.indptr), shape=mixed.shape)
+    check(sp.vstack([single, mixed]).tocsr(), samples, params)
