@@ -133,7 +133,6 @@ struct MinhashCudaGenerator_ {
   // Grow-only workspace.
   mutable DevBuf d_weights, d_cols, d_indptr, d_out, d_chunk_row, d_part_ln, d_part_kt, d_status;
   mutable PinnedBuf h_status;
-  mutable PinnedBuf h_stage;      // batch staging (weights | cols | indptr)
   // Row-block pipeline of mhcuda_calc: two slots, each a block's device CSR,
   // hashes and (for pageable caller buffers) pinned staging.
   struct Slot {
@@ -157,7 +156,7 @@ struct MinhashCudaGenerator_ {
     if (stream) cudaStreamSynchronize(stream);
     d_weights.release(); d_cols.release(); d_indptr.release(); d_out.release();
     d_chunk_row.release(); d_part_ln.release(); d_part_kt.release(); d_status.release();
-    h_status.release(); h_stage.release();
+    h_status.release();
     for (auto &e : prof_events) {
       cudaEventDestroy(e.first);
       cudaEventDestroy(e.second);
@@ -340,6 +339,19 @@ void par_memcpy(void *dst, const void *src, size_t bytes) {
   for (auto &th : pool) th.join();
 }
 
+// Creates the copy streams and slot events of the pipelines on first use.
+cudaError_t batch_streams(const Gen *gen) {
+  if (gen->s_in) return cudaSuccess;
+  cudaError_t e = cudaStreamCreateWithFlags(&gen->s_in, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&gen->s_out, cudaStreamNonBlocking);
+  for (auto &sl : gen->slots) {
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.h2d, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.d2h, cudaEventDisableTiming);
+  }
+  return e;
+}
+
 // Inputs with at least this many nnz go through the row-block pipeline.
 constexpr uint64_t kPipelineMinNnz = 16ull << 20;
 
@@ -351,17 +363,7 @@ constexpr uint64_t kPipelineMinNnz = 16ull << 20;
 MHCUDAResult calc_pipelined(const Gen *gen, const float *weights, const uint32_t *cols,
                             const uint32_t *rows, uint32_t length, uint32_t *output) {
   const cudaStream_t st = gen->stream;
-  if (!gen->s_in) {
-    MHB_CHECK(gen, cudaStreamCreateWithFlags(&gen->s_in, cudaStreamNonBlocking),
-              mhcudaRuntimeError);
-    MHB_CHECK(gen, cudaStreamCreateWithFlags(&gen->s_out, cudaStreamNonBlocking),
-              mhcudaRuntimeError);
-    for (auto &sl : gen->slots) {
-      MHB_CHECK(gen, cudaEventCreateWithFlags(&sl.h2d, cudaEventDisableTiming), mhcudaRuntimeError);
-      MHB_CHECK(gen, cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming), mhcudaRuntimeError);
-      MHB_CHECK(gen, cudaEventCreateWithFlags(&sl.d2h, cudaEventDisableTiming), mhcudaRuntimeError);
-    }
-  }
+  MHB_CHECK(gen, batch_streams(gen), mhcudaRuntimeError);
   const uint64_t nnz = static_cast<uint64_t>(rows[length]) - rows[0];
   uint64_t block_nnz = std::min<uint64_t>(std::max<uint64_t>(nnz / 8, 8ull << 20), 256ull << 20);
   const int forced = env_int("MHCUDA_B200_BLOCK_NNZ", 0);
@@ -742,78 +744,157 @@ enum MHCUDAResult mhcuda_calc_batch(const MinhashCudaGenerator *gen, uint32_t co
   if (!gen || !weights || !cols || !rows || !lengths || !outputs) return mhcudaInvalidArguments;
   std::lock_guard<std::mutex> lock(gen->mu);
   MHB_CHECK(gen, cudaSetDevice(gen->device), mhcudaNoSuchDevice);
-  // Global row / position offsets of each matrix in the staged batch.
-  std::vector<uint64_t> row_off(count + 1, 0), pos_off(count + 1, 0);
+  // Per-matrix nnz; validated before any device work.
+  std::vector<uint64_t> nnz_of(count, 0);
   for (uint32_t i = 0; i < count; ++i) {
-    uint64_t len = lengths[i], n = 0;
-    if (len) {
-      if (!weights[i] || !cols[i] || !rows[i] || !outputs[i]) return mhcudaInvalidArguments;
-      if (rows[i][len] < rows[i][0]) return mhcudaInvalidArguments;
-      n = rows[i][len] - rows[i][0];
-    }
-    row_off[i + 1] = row_off[i] + len;
-    pos_off[i + 1] = pos_off[i] + n;
+    const uint64_t len = lengths[i];
+    if (!len) continue;
+    if (!weights[i] || !cols[i] || !rows[i] || !outputs[i]) return mhcudaInvalidArguments;
+    if (rows[i][len] < rows[i][0]) return mhcudaInvalidArguments;
+    nnz_of[i] = rows[i][len] - rows[i][0];
   }
-  const uint64_t total_rows = row_off[count], total_nnz = pos_off[count];
-  if (total_rows == 0) return mhcudaSuccess;
-  if (total_rows >= 0xFFFFFFFFull || total_nnz >= 0xFFFFFFFFull) return mhcudaInvalidArguments;
+  MHB_CHECK(gen, batch_streams(gen), mhcudaRuntimeError);
   const cudaStream_t st = gen->stream;
-  // Pinned staging: weights | cols | indptr, gathered by a few host threads.
-  const size_t wb = total_nnz * 4, ib = (total_rows + 1) * 4;
-  MHB_CHECK(gen, gen->h_stage.ensure(2 * wb + ib), mhcudaMemoryAllocationFailure);
-  char *stage = gen->h_stage.as<char>();
-  float *sw = reinterpret_cast<float *>(stage);
-  uint32_t *sc = reinterpret_cast<uint32_t *>(stage + wb);
-  uint32_t *si = reinterpret_cast<uint32_t *>(stage + 2 * wb);
+  const size_t row_bytes = static_cast<size_t>(gen->samples) * 2 * sizeof(uint32_t);
+  uint64_t group_nnz = 64ull << 20;
+  const int forced = env_int("MHCUDA_B200_BLOCK_NNZ", 0);
+  if (forced > 0) group_nnz = static_cast<uint64_t>(forced);
+  const uint64_t group_rows = 1u << 20;
+  MHB_CHECK(gen, gen->d_status.ensure(sizeof(uint32_t)), mhcudaMemoryAllocationFailure);
+  MHB_CHECK(gen, cudaMemsetAsync(gen->d_status.ptr, 0, sizeof(uint32_t), st), mhcudaRuntimeError);
   const unsigned nth = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
-  {
+
+  // A slot's staged hashes go back to their matrices once its copy is done.
+  struct Pending {
+    uint32_t first = 0, last = 0;  // matrices [first, last)
+  };
+  Pending pending[2];
+  auto retire = [&](uint32_t k) -> MHCUDAResult {
+    Gen::Slot &sl = gen->slots[k];
+    if (!sl.busy) return mhcudaSuccess;
+    MHB_CHECK(gen, cudaEventSynchronize(sl.d2h), mhcudaMemoryCopyError);
+    const Pending pd = pending[k];
+    const char *src = sl.hout.as<char>();
+    std::vector<size_t> off(pd.last - pd.first + 1, 0);
+    for (uint32_t i = pd.first; i < pd.last; ++i)
+      off[i - pd.first + 1] = off[i - pd.first] + lengths[i] * row_bytes;
     std::vector<std::thread> pool;
     for (unsigned t = 0; t < nth; ++t) {
       pool.emplace_back([&, t]() {
-        for (uint32_t i = t; i < count; i += nth) {
-          const uint64_t len = lengths[i];
-          if (!len) continue;
-          const uint32_t b = rows[i][0];
-          const uint64_t n = pos_off[i + 1] - pos_off[i];
-          memcpy(sw + pos_off[i], weights[i] + b, n * 4);
-          memcpy(sc + pos_off[i], cols[i] + b, n * 4);
-          for (uint64_t r = 0; r < len; ++r)
-            si[row_off[i] + r] = static_cast<uint32_t>(pos_off[i] + (rows[i][r] - b));
-        }
+        for (uint32_t i = pd.first + t; i < pd.last; i += nth)
+          if (lengths[i]) memcpy(outputs[i], src + off[i - pd.first], lengths[i] * row_bytes);
       });
     }
     for (auto &th : pool) th.join();
+    sl.busy = false;
+    return mhcudaSuccess;
+  };
+
+  MHCUDAResult r = mhcudaSuccess;
+  uint32_t m0 = 0;
+  for (uint32_t g = 0; m0 < count && r == mhcudaSuccess; ++g) {
+    // Group [m0, m1): consecutive matrices up to ~group_nnz entries / group_rows rows.
+    uint32_t m1 = m0;
+    uint64_t gn = 0, gr = 0;
+    while (m1 < count) {
+      const uint64_t n = nnz_of[m1], l = lengths[m1];
+      if (m1 > m0 && (gn + n > group_nnz || gr + l > group_rows)) break;
+      if (gn + n >= 0xFFFFFFFFull || gr + l >= 0xFFFFFFFFull) {
+        if (m1 == m0) r = mhcudaInvalidArguments;
+        break;
+      }
+      gn += n;
+      gr += l;
+      ++m1;
+    }
+    if (r != mhcudaSuccess) break;
+    const uint32_t k = g & 1;
+    Gen::Slot &sl = gen->slots[k];
+    r = retire(k);
+    if (r != mhcudaSuccess) break;
+    if (gr == 0) {  // only empty matrices
+      m0 = m1;
+      continue;
+    }
+    const uint32_t R = static_cast<uint32_t>(gr), N = static_cast<uint32_t>(gn);
+    MHB_CHECK(gen, sl.hw.ensure(static_cast<size_t>(N) * 4), mhcudaMemoryAllocationFailure);
+    MHB_CHECK(gen, sl.hc.ensure(static_cast<size_t>(N) * 4), mhcudaMemoryAllocationFailure);
+    MHB_CHECK(gen, sl.hip.ensure((static_cast<size_t>(R) + 1) * 4), mhcudaMemoryAllocationFailure);
+    MHB_CHECK(gen, sl.hout.ensure(static_cast<size_t>(R) * row_bytes), mhcudaMemoryAllocationFailure);
+    MHB_CHECK(gen, sl.w.ensure(static_cast<size_t>(N) * 4 + 16), mhcudaMemoryAllocationFailure);
+    MHB_CHECK(gen, sl.c.ensure(static_cast<size_t>(N) * 4 + 16), mhcudaMemoryAllocationFailure);
+    MHB_CHECK(gen, sl.ip.ensure((static_cast<size_t>(R) + 1) * 4), mhcudaMemoryAllocationFailure);
+    MHB_CHECK(gen, sl.out.ensure(static_cast<size_t>(R) * row_bytes), mhcudaMemoryAllocationFailure);
+    // Gather the group into pinned staging: values and columns back to back,
+    // row offsets rebased to the group's positions.
+    std::vector<uint64_t> moff(m1 - m0 + 1, 0), roff(m1 - m0 + 1, 0);
+    for (uint32_t i = m0; i < m1; ++i) {
+      moff[i - m0 + 1] = moff[i - m0] + nnz_of[i];
+      roff[i - m0 + 1] = roff[i - m0] + lengths[i];
+    }
+    float *sw = sl.hw.as<float>();
+    uint32_t *sc = sl.hc.as<uint32_t>(), *si = sl.hip.as<uint32_t>();
+    {
+      std::vector<std::thread> pool;
+      for (unsigned t = 0; t < nth; ++t) {
+        pool.emplace_back([&, t]() {
+          for (uint32_t i = m0 + t; i < m1; i += nth) {
+            const uint64_t len = lengths[i];
+            if (!len) continue;
+            const uint32_t b = rows[i][0];
+            const uint64_t po = moff[i - m0], ro = roff[i - m0];
+            memcpy(sw + po, weights[i] + b, nnz_of[i] * 4);
+            memcpy(sc + po, cols[i] + b, nnz_of[i] * 4);
+            for (uint64_t x = 0; x < len; ++x)
+              si[ro + x] = static_cast<uint32_t>(po + (rows[i][x] - b));
+          }
+        });
+      }
+      for (auto &th : pool) th.join();
+    }
+    si[R] = N;
+    MHB_CHECK(gen, cudaMemcpyAsync(sl.ip.ptr, si, (static_cast<size_t>(R) + 1) * 4,
+                                   cudaMemcpyHostToDevice, gen->s_in),
+              mhcudaMemoryCopyError);
+    if (N) {
+      MHB_CHECK(gen, cudaMemcpyAsync(sl.w.ptr, sw, static_cast<size_t>(N) * 4,
+                                     cudaMemcpyHostToDevice, gen->s_in),
+                mhcudaMemoryCopyError);
+      MHB_CHECK(gen, cudaMemcpyAsync(sl.c.ptr, sc, static_cast<size_t>(N) * 4,
+                                     cudaMemcpyHostToDevice, gen->s_in),
+                mhcudaMemoryCopyError);
+    }
+    MHB_CHECK(gen, cudaEventRecord(sl.h2d, gen->s_in), mhcudaRuntimeError);
+    MHB_CHECK(gen, cudaStreamWaitEvent(st, sl.h2d, 0), mhcudaRuntimeError);
+    const HashPlan plan = make_plan(gen, N, R);
+    HashArgs a{};
+    r = prepare_launch(gen, R, N, plan, &a);
+    if (r != mhcudaSuccess) break;
+    a.weights = sl.w.as<float>();
+    a.cols = sl.c.as<uint32_t>();
+    a.indptr = sl.ip.as<uint32_t>();
+    a.out = sl.out.as<uint32_t>();
+    r = enqueue_hash(gen, a, plan, st, /*clear_status=*/false);
+    if (r != mhcudaSuccess) break;
+    MHB_CHECK(gen, cudaEventRecord(sl.done, st), mhcudaRuntimeError);
+    MHB_CHECK(gen, cudaStreamWaitEvent(gen->s_out, sl.done, 0), mhcudaRuntimeError);
+    MHB_CHECK(gen, cudaMemcpyAsync(sl.hout.ptr, sl.out.ptr, static_cast<size_t>(R) * row_bytes,
+                                   cudaMemcpyDeviceToHost, gen->s_out),
+              mhcudaMemoryCopyError);
+    MHB_CHECK(gen, cudaEventRecord(sl.d2h, gen->s_out), mhcudaRuntimeError);
+    sl.busy = true;
+    sl.pending_out = nullptr;
+    pending[k] = Pending{m0, m1};
+    MHB_DEBUG(gen, "batch group %u: matrices [%u, %u) rows %u nnz %u\n", g, m0, m1, R, N);
+    m0 = m1;
   }
-  si[total_rows] = static_cast<uint32_t>(total_nnz);
-  const uint32_t nnz = static_cast<uint32_t>(total_nnz), R = static_cast<uint32_t>(total_rows);
-  MHB_CHECK(gen, gen->d_weights.ensure(wb + 16), mhcudaMemoryAllocationFailure);
-  MHB_CHECK(gen, gen->d_cols.ensure(wb + 16), mhcudaMemoryAllocationFailure);
-  MHB_CHECK(gen, gen->d_indptr.ensure(ib), mhcudaMemoryAllocationFailure);
-  const size_t row_bytes = static_cast<size_t>(gen->samples) * 2 * sizeof(uint32_t);
-  MHB_CHECK(gen, gen->d_out.ensure(total_rows * row_bytes), mhcudaMemoryAllocationFailure);
-  if (wb) {
-    MHB_CHECK(gen, cudaMemcpyAsync(gen->d_weights.ptr, sw, wb, cudaMemcpyHostToDevice, st),
-              mhcudaMemoryCopyError);
-    MHB_CHECK(gen, cudaMemcpyAsync(gen->d_cols.ptr, sc, wb, cudaMemcpyHostToDevice, st),
-              mhcudaMemoryCopyError);
+  for (uint32_t k = 0; k < 2; ++k) {
+    const MHCUDAResult rr = retire(k);
+    if (r == mhcudaSuccess) r = rr;
   }
-  MHB_CHECK(gen, cudaMemcpyAsync(gen->d_indptr.ptr, si, ib, cudaMemcpyHostToDevice, st),
-            mhcudaMemoryCopyError);
-  const HashPlan plan = make_plan(gen, nnz, R);
-  HashArgs a{};
-  MHCUDAResult r = prepare_launch(gen, R, nnz, plan, &a);
-  if (r != mhcudaSuccess) return r;
-  a.weights = gen->d_weights.as<float>();
-  a.cols = gen->d_cols.as<uint32_t>();
-  a.indptr = gen->d_indptr.as<uint32_t>();
-  a.out = gen->d_out.as<uint32_t>();
-  r = enqueue_hash(gen, a, plan, st);
-  if (r != mhcudaSuccess) return r;
-  for (uint32_t i = 0; i < count; ++i) {
-    if (!lengths[i]) continue;
-    MHB_CHECK(gen, cudaMemcpyAsync(outputs[i], gen->d_out.as<char>() + row_off[i] * row_bytes,
-                                   lengths[i] * row_bytes, cudaMemcpyDeviceToHost, st),
-              mhcudaMemoryCopyError);
+  if (r != mhcudaSuccess) {
+    cudaDeviceSynchronize();
+    return r;
   }
   return read_status(gen, st);
 }

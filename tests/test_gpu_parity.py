@@ -251,3 +251,37 @@ def test_near_integer_quotients():
     mixed = random_csr(rng, 500, dim, 40)
     mixed = sp.csr_matrix((wt[mixed.indices], mixed.indices, mixed.indptr), shape=mixed.shape)
     check(sp.vstack([single, mixed]).tocsr(), samples, params)
+
+
+@pytest.mark.parametrize("group_nnz", [1500, 20000])
+def test_batch_groups_and_empty_matrices(monkeypatch, group_nnz):
+    """mhcuda_calc_batch cut into several pipelined groups (including empty
+    matrices and matrices larger than a group) equals one calc per matrix."""
+    import ctypes
+    rng = np.random.default_rng(group_nnz)
+    dim, samples = 3000, 64
+    params = gamma_params(rng, dim, samples)
+    mats = []
+    for i in range(60):
+        rows = int(rng.integers(0, 120)) if i % 7 else 0
+        mats.append(random_csr(rng, rows, dim, float(rng.integers(1, 90)),
+                               long_rows=[(0, 2500)] if rows and i % 11 == 0 else ()))
+    co = O.COracle(*params)
+    with engine_gen(dim, samples, deferred=True) as eng:
+        eng.assign(*params)
+        monkeypatch.setenv("MHCUDA_B200_BLOCK_NNZ", str(group_nnz))
+        arrs = [(m.data.astype(np.float32), m.indices.astype(np.uint32),
+                 m.indptr.astype(np.uint32)) for m in mats]
+        outs = [np.full((m.shape[0], samples, 2), 3, np.uint32) for m in mats]
+        P = ctypes.c_void_p
+        W = (P * len(mats))(*[a[0].ctypes.data for a in arrs])
+        C = (P * len(mats))(*[a[1].ctypes.data for a in arrs])
+        R = (P * len(mats))(*[a[2].ctypes.data for a in arrs])
+        L = (ctypes.c_uint32 * len(mats))(*[m.shape[0] for m in mats])
+        OUT = (P * len(mats))(*[o.ctypes.data for o in outs])
+        for _ in range(2):  # twice: slots and staging are reused
+            rc = eng.lib.mhcuda_calc_batch(eng.h, len(mats), W, C, R, L, OUT)
+            assert rc == 0
+            for m, o in zip(mats, outs):
+                if m.shape[0]:
+                    np.testing.assert_array_equal(o, co.hash_csr(m, lnw=device_logf(m.data)))
