@@ -96,6 +96,55 @@ enum MHCUDAResult mhcuda_profile(const MinhashCudaGenerator *gen, int enable);
 enum MHCUDAResult mhcuda_profile_read(const MinhashCudaGenerator *gen, double *hash_ms,
                                       uint64_t *launches);
 
+/* ---- Serving: a continuous-batching request loop on one device ----------
+ * No counterpart in the reference (every mhcuda_calc there is one blocking
+ * launch per device, minhashcuda.cc:583-642).  A worker thread keeps `lanes`
+ * batches in flight on separate streams; each request (a CSR and an output
+ * buffer in host memory, as for mhcuda_calc, hashed against any generator on
+ * the server's device) is cut into row blocks that fit a lane, and free lanes
+ * take the oldest waiting blocks of one generator at a time.  Requests that
+ * arrive while others run start as soon as a lane frees up.  Device memory
+ * used by the server is `hbm_budget_bytes` (split between the lanes at start;
+ * nothing grows later).  Results are bit-identical to mhcuda_calc. */
+typedef struct MinhashCudaServer_ MinhashCudaServer;
+
+/* Starts a server on the device selected like mhcuda_init's `devices`.
+ * lanes: 1..16; hbm_budget_bytes >= 64 MiB. */
+MinhashCudaServer *mhcuda_server_start(uint32_t devices, uint64_t hbm_budget_bytes,
+                                       uint32_t lanes, int verbosity,
+                                       enum MHCUDAResult *status);
+
+/* Queues a request and returns its ticket.  The host buffers must stay valid
+ * and unmodified until the request is waited for.  Refused with
+ * mhcudaMemoryAllocationFailure if one row alone does not fit a lane. */
+enum MHCUDAResult mhcuda_server_submit(MinhashCudaServer *srv, const MinhashCudaGenerator *gen,
+                                       const float *weights, const uint32_t *cols,
+                                       const uint32_t *rows, uint32_t length, uint32_t *output,
+                                       uint64_t *ticket);
+
+/* *done = 1 once the request's hashes are in its output buffer. */
+enum MHCUDAResult mhcuda_server_poll(MinhashCudaServer *srv, uint64_t ticket, int *done);
+
+/* Waits up to timeout_s for the request, then returns its result
+ * (mhcudaInvalidArguments for invalid CSR, mhcudaRuntimeError if cancelled
+ * or timed out) and, if latency_ms is not NULL, its submit-to-done time.
+ * A finished ticket is released by this call. */
+enum MHCUDAResult mhcuda_server_wait(MinhashCudaServer *srv, uint64_t ticket, double timeout_s,
+                                     double *latency_ms);
+
+/* Drops the request's blocks that have not started; it then completes with
+ * mhcudaRuntimeError. */
+enum MHCUDAResult mhcuda_server_cancel(MinhashCudaServer *srv, uint64_t ticket);
+
+/* Latency percentiles over completed requests and hashed nnz*samples per
+ * second since start or the last reset. */
+enum MHCUDAResult mhcuda_server_stats(MinhashCudaServer *srv, int reset, uint64_t *completed,
+                                      double *p50_ms, double *p99_ms, double *p999_ms,
+                                      double *evals_per_s);
+
+/* Finishes queued work and frees the server. */
+enum MHCUDAResult mhcuda_server_stop(MinhashCudaServer *srv);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif

@@ -66,6 +66,18 @@ SIGNATURES = {
     "mhcuda_calc_device_noalloc": (_RES, [_P, _P, _P, _P, _U32, _U32, _P, _P]),
     "mhcuda_calc_batch": (_RES, [_P, _U32, _P, _P, _P, _P, _P]),
     "mhcuda_debug_device_logf": (_RES, [_U32, _P, _P, ctypes.c_uint64]),
+    "mhcuda_server_start": (_P, [_U32, ctypes.c_uint64, _U32, ctypes.c_int,
+                                 ctypes.POINTER(ctypes.c_int)]),
+    "mhcuda_server_submit": (_RES, [_P, _P, _P, _P, _P, _U32, _P,
+                                    ctypes.POINTER(ctypes.c_uint64)]),
+    "mhcuda_server_poll": (_RES, [_P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int)]),
+    "mhcuda_server_wait": (_RES, [_P, ctypes.c_uint64, ctypes.c_double,
+                                  ctypes.POINTER(ctypes.c_double)]),
+    "mhcuda_server_cancel": (_RES, [_P, ctypes.c_uint64]),
+    "mhcuda_server_stats": (_RES, [_P, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64),
+                                   ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                   ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    "mhcuda_server_stop": (_RES, [_P]),
     "mhcuda_profile": (_RES, [_P, ctypes.c_int]),
     "mhcuda_profile_read": (_RES, [_P, ctypes.POINTER(ctypes.c_double),
                                    ctypes.POINTER(ctypes.c_uint64)]),

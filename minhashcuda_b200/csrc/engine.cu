@@ -517,6 +517,10 @@ MHCUDAResult init_params(Gen *gen, uint32_t seed) {
 
 namespace mhb {
 
+HashPlan plan_for_generator(const MinhashCudaGenerator_ *gen, uint64_t nnz, uint64_t rows) {
+  return make_plan(gen, nnz, rows);
+}
+
 bool generator_view(const MinhashCudaGenerator_ *gen, GeneratorView *view) {
   if (!gen || !view) return false;
   view->params = gen->params;

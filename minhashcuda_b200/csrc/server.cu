@@ -1,0 +1,604 @@
+// Continuous-batching hash server (mhcuda_server_*).
+//
+// The reference has no server: every mhcuda_calc call is one synchronous
+// launch per device (minhashcuda.cc:583-642).  Here a worker thread keeps
+// several "lanes" busy on one device.  Each lane owns a CUDA stream, device
+// buffers for one batch (CSR in, hashes out, chunk scratch) and pinned host
+// staging.  Requests are cut into row-range units small enough for a lane;
+// whenever a lane is free it takes the oldest pending unit and every
+// following unit of the same generator that still fits, gathers them into
+// one CSR, and runs copy-in, the plan/hash/finalize kernels and copy-out on
+// its stream.  Lanes run concurrently, so a request that arrives while other
+// batches are on the GPU starts as soon as a lane frees up and its work
+// overlaps theirs.  Device memory is bounded by the budget given at start:
+// the lanes are sized from it once and nothing grows afterwards.
+//
+// Per-request guarantees: the hashes equal a lone mhcuda_calc of the same
+// request bit for bit (same kernels, same per-row arithmetic; the batch only
+// changes which warp walks which positions).  A batch whose device status
+// reports invalid CSR is re-run unit by unit so that only the offending
+// request fails.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/minhashcuda.h"
+#include "../../include/minhashcuda_b200.h"
+#include "wmh_internal.h"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+  uint64_t ticket = 0;
+  const MinhashCudaGenerator_ *gen = nullptr;
+  mhb::GeneratorView g{};
+  const float *weights = nullptr;
+  const uint32_t *cols = nullptr;
+  const uint32_t *rows = nullptr;
+  uint32_t length = 0;
+  uint32_t *output = nullptr;
+  Clock::time_point submitted, finished;
+  uint32_t units_left = 0;
+  MHCUDAResult result = mhcudaSuccess;
+  bool cancelled = false;
+  bool done = false;
+};
+
+struct Unit {
+  Request *req;
+  uint32_t r0, r1;  // rows of the request
+};
+
+struct Lane {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done_ev = nullptr;
+  // device
+  float *w = nullptr;
+  uint32_t *c = nullptr, *ip = nullptr, *out = nullptr, *chunk_row = nullptr, *status = nullptr;
+  float *part_ln = nullptr;
+  uint2 *part_kt = nullptr;
+  // pinned host
+  float *hw = nullptr;
+  uint32_t *hc = nullptr, *hip = nullptr, *hout = nullptr, *hstatus = nullptr;
+  std::vector<Unit> units;
+  std::vector<uint64_t> unit_rows;  // row offset of each unit inside the batch
+  bool busy = false;
+};
+
+size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
+
+}  // namespace
+
+struct MinhashCudaServer_ {
+  int device = 0;
+  int verbosity = 0;
+  int sm_count = 148;
+  // Per-lane capacities (bytes).
+  size_t in_cap = 0, out_cap = 0, scratch_cap = 0;
+  size_t scratch_unit = 0;  // scratch = chunk_row (1 unit) | part_ln (4) | part_kt (8)
+  std::vector<Lane> lanes;
+
+  std::mutex mu;
+  std::condition_variable wake;       // worker: new work or a lane finished
+  std::condition_variable finished;   // waiters: a request completed
+  std::deque<Request *> incoming;     // submitted, not yet cut into units
+  std::deque<Unit> pending;           // units waiting for a lane
+  std::unordered_map<uint64_t, std::unique_ptr<Request>> requests;
+  std::vector<double> latencies_ms;   // completed requests, for mhcuda_server_stats
+  uint64_t next_ticket = 1;
+  uint64_t evals_done = 0;
+  Clock::time_point stats_since = Clock::now();
+  bool stop = false;
+  std::atomic<int> signals{0};
+  std::thread worker;
+
+  ~MinhashCudaServer_();
+  void run();
+  bool take(Lane &lane);
+  void start(Lane &lane);
+  void complete(Lane &lane);
+  MHCUDAResult run_units(Lane &lane, const std::vector<Unit> &units, bool solo);
+  size_t unit_in_bytes(const Unit &u) const {
+    const uint64_t n = static_cast<uint64_t>(u.req->rows[u.r1]) - u.req->rows[u.r0];
+    return n * 8 + (static_cast<size_t>(u.r1 - u.r0) + 1) * 4;
+  }
+  size_t unit_out_bytes(const Unit &u) const {
+    return static_cast<size_t>(u.r1 - u.r0) * u.req->g.samples * 8;
+  }
+};
+
+namespace {
+
+void CUDART_CB notify_worker(void *p) {
+  auto *srv = static_cast<MinhashCudaServer_ *>(p);
+  srv->signals.fetch_add(1);
+  srv->wake.notify_one();
+}
+
+void par_copy(void *dst, const void *src, size_t bytes) {
+  const size_t kSplit = static_cast<size_t>(16) << 20;
+  if (bytes < kSplit) {
+    memcpy(dst, src, bytes);
+    return;
+  }
+  const unsigned n = std::min(8u, std::max(1u, std::thread::hardware_concurrency()));
+  const size_t part = (((bytes + n - 1) / n) + 4095) & ~static_cast<size_t>(4095);
+  std::vector<std::thread> pool;
+  for (unsigned t = 0; t < n; ++t) {
+    const size_t off = t * part;
+    if (off >= bytes) break;
+    const size_t len = std::min(part, bytes - off);
+    pool.emplace_back([=]() {
+      memcpy(static_cast<char *>(dst) + off, static_cast<const char *>(src) + off, len);
+    });
+  }
+  for (auto &th : pool) th.join();
+}
+
+}  // namespace
+
+MinhashCudaServer_::~MinhashCudaServer_() {
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    stop = true;
+  }
+  wake.notify_all();
+  if (worker.joinable()) worker.join();
+  cudaSetDevice(device);
+  for (Lane &l : lanes) {
+    if (l.stream) cudaStreamSynchronize(l.stream);
+    cudaFree(l.w);
+    cudaFree(l.c);
+    cudaFree(l.ip);
+    cudaFree(l.out);
+    cudaFree(l.chunk_row);  // base of the scratch that also holds part_ln / part_kt
+    cudaFree(l.status);
+    cudaFreeHost(l.hw);
+    cudaFreeHost(l.hc);
+    cudaFreeHost(l.hip);
+    cudaFreeHost(l.hout);
+    cudaFreeHost(l.hstatus);
+    if (l.done_ev) cudaEventDestroy(l.done_ev);
+    if (l.stream) cudaStreamDestroy(l.stream);
+  }
+}
+
+// Gathers `units` into the lane's staging and enqueues copy-in, kernels and
+// copy-out on the lane's stream.  With `solo` the call waits for the result
+// (used to attribute an invalid-CSR status to single units).
+MHCUDAResult MinhashCudaServer_::run_units(Lane &lane, const std::vector<Unit> &units, bool solo) {
+  const mhb::GeneratorView &g = units.front().req->g;
+  uint64_t R = 0, N = 0;
+  lane.unit_rows.assign(units.size() + 1, 0);
+  std::vector<uint64_t> pos(units.size() + 1, 0);
+  for (size_t k = 0; k < units.size(); ++k) {
+    const Unit &u = units[k];
+    R += u.r1 - u.r0;
+    N += static_cast<uint64_t>(u.req->rows[u.r1]) - u.req->rows[u.r0];
+    lane.unit_rows[k + 1] = R;
+    pos[k + 1] = N;
+  }
+  for (size_t k = 0; k < units.size(); ++k) {
+    const Unit &u = units[k];
+    const uint32_t b = u.req->rows[u.r0];
+    const uint64_t n = pos[k + 1] - pos[k];
+    par_copy(lane.hw + pos[k], u.req->weights + b, n * 4);
+    par_copy(lane.hc + pos[k], u.req->cols + b, n * 4);
+    uint32_t *ip = lane.hip + lane.unit_rows[k];
+    for (uint32_t x = u.r0; x < u.r1; ++x) ip[x - u.r0] = static_cast<uint32_t>(pos[k] + (u.req->rows[x] - b));
+  }
+  lane.hip[R] = static_cast<uint32_t>(N);
+  const cudaStream_t st = lane.stream;
+  const uint32_t s_pad = g.s_pad;
+  mhb::HashPlan plan = mhb::plan_for_generator(units.front().req->gen, N, R);
+  // Keep the chunk table and partials inside the lane's fixed scratch:
+  // nchunks*4 <= unit, 2*nchunks*s_pad*4 <= 4*unit, 2*nchunks*s_pad*8 <= 8*unit.
+  const uint64_t max_chunks = std::max<uint64_t>(
+      1, std::min<uint64_t>(scratch_unit / 4, scratch_unit / (2 * static_cast<uint64_t>(s_pad))));
+  if (N > static_cast<uint64_t>(plan.chunk) * max_chunks) {
+    uint64_t chunk = (N + max_chunks - 1) / max_chunks;
+    chunk = (chunk + 31) & ~31ull;
+    plan.chunk = static_cast<uint32_t>(chunk);
+    plan.nchunks = static_cast<uint32_t>((N + chunk - 1) / chunk);
+    const uint64_t items = static_cast<uint64_t>(plan.nchunks) * plan.ntiles;
+    const int bps = mhb::hash_blocks_per_sm(plan.spl, plan.minb);
+    plan.grid = static_cast<uint32_t>(std::max<uint64_t>(
+        1, std::min<uint64_t>((items + 7) / 8, static_cast<uint64_t>(sm_count) * bps)));
+  }
+  mhb::HashArgs a{};
+  a.params = g.params;
+  a.dim = g.dim;
+  a.samples = g.samples;
+  a.s_pad = s_pad;
+  a.weights = lane.w;
+  a.cols = lane.c;
+  a.indptr = lane.ip;
+  a.rows = static_cast<uint32_t>(R);
+  a.nnz = static_cast<uint32_t>(N);
+  a.chunk = plan.chunk;
+  a.nchunks = plan.nchunks;
+  a.ntiles = plan.ntiles;
+  a.chunk_row = lane.chunk_row;
+  a.part_ln = lane.part_ln;
+  a.part_kt = lane.part_kt;
+  a.out = lane.out;
+  a.status = lane.status;
+  cudaError_t e = cudaMemcpyAsync(lane.ip, lane.hip, (R + 1) * 4, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && N) e = cudaMemcpyAsync(lane.w, lane.hw, N * 4, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && N) e = cudaMemcpyAsync(lane.c, lane.hc, N * 4, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(lane.status, 0, 4, st);
+  if (e == cudaSuccess) e = mhb::launch_plan(a, st);
+  if (e == cudaSuccess) e = mhb::launch_hash(a, plan, st);
+  if (e == cudaSuccess && plan.nchunks > 1) e = mhb::launch_finalize(a, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(lane.hout, lane.out, R * g.samples * 8, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(lane.hstatus, lane.status, 4, cudaMemcpyDeviceToHost, st);
+  // The event is recorded before the wake-up callback so the worker finds it
+  // complete when the callback wakes it.
+  if (e == cudaSuccess) e = cudaEventRecord(lane.done_ev, st);
+  if (e == cudaSuccess && !solo) e = cudaLaunchHostFunc(st, notify_worker, this);
+  if (e == cudaSuccess && solo) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return mhcudaRuntimeError;
+  }
+  return mhcudaSuccess;
+}
+
+// Under `mu`: moves the oldest pending unit and every later unit of the same
+// generator that still fits the lane (bounded look-ahead keeps admission
+// close to FIFO) into lane.units.  Returns false if nothing was taken.
+bool MinhashCudaServer_::take(Lane &lane) {
+  std::vector<Unit> batch;
+  size_t in = 0, out = 0;
+  const MinhashCudaGenerator_ *gen = nullptr;
+  size_t scanned = 0;
+  for (auto it = pending.begin(); it != pending.end() && scanned < 512; ++scanned) {
+    if (it->req->cancelled) {
+      Request *r = it->req;
+      it = pending.erase(it);
+      if (--r->units_left == 0 && !r->done) {
+        r->done = true;
+        r->finished = Clock::now();
+        finished.notify_all();
+      }
+      continue;
+    }
+    if (gen && it->req->gen != gen) {
+      ++it;
+      continue;
+    }
+    const size_t ui = unit_in_bytes(*it), uo = unit_out_bytes(*it);
+    if (!batch.empty() && (in + ui > in_cap || out + uo > out_cap)) break;
+    gen = it->req->gen;
+    in += ui;
+    out += uo;
+    batch.push_back(*it);
+    it = pending.erase(it);
+  }
+  if (batch.empty()) return false;
+  lane.units = std::move(batch);
+  lane.busy = true;
+  return true;
+}
+
+// Without `mu`: gathers and enqueues the lane's batch.
+void MinhashCudaServer_::start(Lane &lane) {
+  const MHCUDAResult r = run_units(lane, lane.units, false);
+  if (r == mhcudaSuccess) return;
+  std::lock_guard<std::mutex> lock(mu);
+  const Clock::time_point now = Clock::now();
+  for (const Unit &u : lane.units) {
+    u.req->result = r;
+    if (--u.req->units_left == 0) {
+      u.req->done = true;
+      u.req->finished = now;
+    }
+  }
+  lane.units.clear();
+  lane.busy = false;
+  finished.notify_all();
+}
+
+void MinhashCudaServer_::complete(Lane &lane) {
+  std::vector<Unit> units = std::move(lane.units);
+  std::vector<MHCUDAResult> unit_result(units.size(), mhcudaSuccess);
+  if (*lane.hstatus != 0) {
+    // Attribute the invalid input: run every unit of the batch on its own.
+    for (size_t k = 0; k < units.size(); ++k) {
+      std::vector<Unit> one{units[k]};
+      unit_result[k] = run_units(lane, one, true);
+      if (unit_result[k] == mhcudaSuccess && *lane.hstatus != 0)
+        unit_result[k] = mhcudaInvalidArguments;
+      if (unit_result[k] == mhcudaSuccess) {
+        const Unit &u = units[k];
+        par_copy(u.req->output + static_cast<size_t>(u.r0) * u.req->g.samples * 2, lane.hout,
+                 unit_out_bytes(u));
+      }
+    }
+  } else {
+    for (size_t k = 0; k < units.size(); ++k) {
+      const Unit &u = units[k];
+      par_copy(u.req->output + static_cast<size_t>(u.r0) * u.req->g.samples * 2,
+               lane.hout + lane.unit_rows[k] * u.req->g.samples * 2, unit_out_bytes(u));
+    }
+  }
+  lane.busy = false;
+  std::lock_guard<std::mutex> lock(mu);
+  const Clock::time_point now = Clock::now();
+  for (size_t k = 0; k < units.size(); ++k) {
+    Request *r = units[k].req;
+    evals_done += (static_cast<uint64_t>(r->rows[units[k].r1]) - r->rows[units[k].r0]) * r->g.samples;
+    if (unit_result[k] != mhcudaSuccess) r->result = unit_result[k];
+    if (--r->units_left == 0) {
+      r->done = true;
+      r->finished = now;
+      if (!r->cancelled)
+        latencies_ms.push_back(std::chrono::duration<double, std::milli>(now - r->submitted).count());
+    }
+  }
+  finished.notify_all();
+}
+
+void MinhashCudaServer_::run() {
+  cudaSetDevice(device);
+  const size_t max_rows_unit = 1u << 20;
+  for (;;) {
+    {
+      std::unique_lock<std::mutex> lock(mu);
+      // Cut new requests into units that fit a lane.
+      while (!incoming.empty()) {
+        Request *r = incoming.front();
+        incoming.pop_front();
+        const size_t row_out = static_cast<size_t>(r->g.samples) * 8;
+        uint32_t r0 = 0;
+        while (r0 < r->length) {
+          uint32_t r1 = r0;
+          size_t in = 4, outb = 0;
+          while (r1 < r->length) {
+            const size_t add_in = (static_cast<size_t>(r->rows[r1 + 1]) - r->rows[r1]) * 8 + 4;
+            if (r1 > r0 && (in + add_in > in_cap || outb + row_out > out_cap ||
+                            r1 - r0 >= max_rows_unit))
+              break;
+            in += add_in;
+            outb += row_out;
+            ++r1;
+          }
+          pending.push_back(Unit{r, r0, r1});
+          ++r->units_left;
+          r0 = r1;
+        }
+      }
+      bool any_busy = false;
+      for (const Lane &l : lanes) any_busy |= l.busy;
+      if (stop && !any_busy && pending.empty()) break;
+    }
+    bool progressed = false;
+    for (Lane &l : lanes) {
+      if (l.busy && cudaEventQuery(l.done_ev) == cudaSuccess) {
+        complete(l);
+        progressed = true;
+      }
+    }
+    std::vector<Lane *> taken;
+    {
+      std::lock_guard<std::mutex> lock(mu);
+      for (Lane &l : lanes)
+        if (!l.busy && !pending.empty() && take(l)) taken.push_back(&l);
+    }
+    for (Lane *l : taken) start(*l);
+    progressed |= !taken.empty();
+    {
+      std::unique_lock<std::mutex> lock(mu);
+      if (!progressed && incoming.empty()) {
+        const int seen = signals.load();
+        wake.wait_for(lock, std::chrono::microseconds(200),
+                      [&] { return stop || !incoming.empty() || signals.load() != seen; });
+      }
+    }
+  }
+}
+
+extern "C" {
+
+MinhashCudaServer *mhcuda_server_start(uint32_t devices, uint64_t hbm_budget_bytes, uint32_t lanes,
+                                       int verbosity, enum MHCUDAResult *status) {
+  auto set = [&](MHCUDAResult r) {
+    if (status) *status = r;
+  };
+  if (lanes == 0 || lanes > 16 || hbm_budget_bytes < (static_cast<uint64_t>(64) << 20)) {
+    set(mhcudaInvalidArguments);
+    return nullptr;
+  }
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) {
+    cudaGetLastError();
+    set(mhcudaNoSuchDevice);
+    return nullptr;
+  }
+  int dev = -1;
+  if (devices == 0) dev = 0;
+  for (int d = 0; d < 32 && d < count && dev < 0; ++d)
+    if (devices & (1u << d)) dev = d;
+  if (dev < 0 || cudaSetDevice(dev) != cudaSuccess) {
+    cudaGetLastError();
+    set(mhcudaNoSuchDevice);
+    return nullptr;
+  }
+  std::unique_ptr<MinhashCudaServer_> srv(new MinhashCudaServer_());
+  srv->device = dev;
+  srv->verbosity = verbosity;
+  cudaDeviceGetAttribute(&srv->sm_count, cudaDevAttrMultiProcessorCount, dev);
+  const size_t per_lane = hbm_budget_bytes / lanes;
+  srv->in_cap = align256(per_lane * 4 / 10);
+  srv->out_cap = align256(per_lane * 4 / 10);
+  srv->scratch_cap = align256(per_lane - srv->in_cap - srv->out_cap);
+  srv->scratch_unit = (srv->scratch_cap / 13) & ~static_cast<size_t>(255);
+  srv->lanes.resize(lanes);
+  for (Lane &l : srv->lanes) {
+    const size_t max_nnz = srv->in_cap / 8;
+    bool ok = cudaStreamCreateWithFlags(&l.stream, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&l.done_ev, cudaEventDisableTiming) == cudaSuccess &&
+              cudaMalloc(&l.w, max_nnz * 4 + 16) == cudaSuccess &&
+              cudaMalloc(&l.c, max_nnz * 4 + 16) == cudaSuccess &&
+              cudaMalloc(&l.ip, srv->in_cap + 256) == cudaSuccess &&
+              cudaMalloc(&l.out, srv->out_cap) == cudaSuccess &&
+              cudaMalloc(&l.status, 256) == cudaSuccess &&
+              cudaHostAlloc(reinterpret_cast<void **>(&l.hw), max_nnz * 4 + 16, 0) == cudaSuccess &&
+              cudaHostAlloc(reinterpret_cast<void **>(&l.hc), max_nnz * 4 + 16, 0) == cudaSuccess &&
+              cudaHostAlloc(reinterpret_cast<void **>(&l.hip), srv->in_cap + 256, 0) == cudaSuccess &&
+              cudaHostAlloc(reinterpret_cast<void **>(&l.hout), srv->out_cap, 0) == cudaSuccess &&
+              cudaHostAlloc(reinterpret_cast<void **>(&l.hstatus), 256, 0) == cudaSuccess;
+    // Scratch: chunk table then partial minima, carved from one allocation.
+    char *scratch = nullptr;
+    ok = ok && cudaMalloc(&scratch, srv->scratch_cap) == cudaSuccess;
+    if (!ok) {
+      cudaGetLastError();
+      if (scratch) cudaFree(scratch);
+      set(mhcudaMemoryAllocationFailure);
+      return nullptr;
+    }
+    // Layout within scratch is decided per batch from s_pad; keep the three
+    // pointers at fixed fractions: chunk_row | part_ln | part_kt (1 : 4 : 8).
+    const size_t unit = srv->scratch_unit;
+    l.chunk_row = reinterpret_cast<uint32_t *>(scratch);
+    l.part_ln = reinterpret_cast<float *>(scratch + unit);
+    l.part_kt = reinterpret_cast<uint2 *>(scratch + 5 * unit);
+  }
+  srv->worker = std::thread([s = srv.get()]() { s->run(); });
+  set(mhcudaSuccess);
+  return srv.release();
+}
+
+enum MHCUDAResult mhcuda_server_submit(MinhashCudaServer *srv, const MinhashCudaGenerator *gen,
+                                       const float *weights, const uint32_t *cols,
+                                       const uint32_t *rows, uint32_t length, uint32_t *output,
+                                       uint64_t *ticket) {
+  if (!srv || !gen || !weights || !cols || !rows || !output || !ticket || length == 0)
+    return mhcudaInvalidArguments;
+  std::unique_ptr<Request> r(new Request());
+  if (!mhb::generator_view(gen, &r->g)) return mhcudaInvalidArguments;
+  if (r->g.device != srv->device) return mhcudaNoSuchDevice;
+  if (rows[length] < rows[0]) return mhcudaInvalidArguments;
+  // A single row (and one chunk's partials) must fit a lane on its own.
+  const size_t row_out = static_cast<size_t>(r->g.samples) * 8;
+  if (row_out > srv->out_cap || srv->scratch_unit < 2 * static_cast<size_t>(r->g.s_pad))
+    return mhcudaMemoryAllocationFailure;
+  for (uint32_t i = 0; i < length; ++i) {
+    if (rows[i + 1] < rows[i]) return mhcudaInvalidArguments;
+    if ((static_cast<size_t>(rows[i + 1]) - rows[i]) * 8 + 8 > srv->in_cap)
+      return mhcudaMemoryAllocationFailure;
+  }
+  r->gen = gen;
+  r->weights = weights;
+  r->cols = cols;
+  r->rows = rows;
+  r->length = length;
+  r->output = output;
+  r->submitted = Clock::now();
+  {
+    std::lock_guard<std::mutex> lock(srv->mu);
+    if (srv->stop) return mhcudaRuntimeError;
+    r->ticket = srv->next_ticket++;
+    *ticket = r->ticket;
+    srv->incoming.push_back(r.get());
+    srv->requests.emplace(r->ticket, std::move(r));
+  }
+  srv->wake.notify_one();
+  return mhcudaSuccess;
+}
+
+enum MHCUDAResult mhcuda_server_poll(MinhashCudaServer *srv, uint64_t ticket, int *done) {
+  if (!srv || !done) return mhcudaInvalidArguments;
+  std::lock_guard<std::mutex> lock(srv->mu);
+  auto it = srv->requests.find(ticket);
+  if (it == srv->requests.end()) return mhcudaInvalidArguments;
+  *done = it->second->done ? 1 : 0;
+  return mhcudaSuccess;
+}
+
+enum MHCUDAResult mhcuda_server_wait(MinhashCudaServer *srv, uint64_t ticket, double timeout_s,
+                                     double *latency_ms) {
+  if (!srv) return mhcudaInvalidArguments;
+  std::unique_lock<std::mutex> lock(srv->mu);
+  auto it = srv->requests.find(ticket);
+  if (it == srv->requests.end()) return mhcudaInvalidArguments;
+  Request *r = it->second.get();
+  const auto deadline = Clock::now() + std::chrono::duration_cast<Clock::duration>(
+                                           std::chrono::duration<double>(timeout_s));
+  while (!r->done) {
+    if (srv->finished.wait_until(lock, deadline) == std::cv_status::timeout && !r->done)
+      return mhcudaRuntimeError;
+  }
+  const MHCUDAResult res = r->result;
+  if (latency_ms)
+    *latency_ms = std::chrono::duration<double, std::milli>(r->finished - r->submitted).count();
+  srv->requests.erase(it);
+  return res;
+}
+
+enum MHCUDAResult mhcuda_server_cancel(MinhashCudaServer *srv, uint64_t ticket) {
+  if (!srv) return mhcudaInvalidArguments;
+  std::lock_guard<std::mutex> lock(srv->mu);
+  auto it = srv->requests.find(ticket);
+  if (it == srv->requests.end()) return mhcudaInvalidArguments;
+  Request *r = it->second.get();
+  if (r->done) return mhcudaInvalidArguments;
+  r->cancelled = true;
+  r->result = mhcudaRuntimeError;  // its hashes are not (all) computed
+  // Still in the incoming queue: drop it now.
+  auto q = std::find(srv->incoming.begin(), srv->incoming.end(), r);
+  if (q != srv->incoming.end()) {
+    srv->incoming.erase(q);
+    r->done = true;
+    r->result = mhcudaRuntimeError;
+    r->finished = Clock::now();
+    srv->finished.notify_all();
+  }
+  srv->wake.notify_one();
+  return mhcudaSuccess;
+}
+
+enum MHCUDAResult mhcuda_server_stats(MinhashCudaServer *srv, int reset, uint64_t *completed,
+                                      double *p50_ms, double *p99_ms, double *p999_ms,
+                                      double *evals_per_s) {
+  if (!srv) return mhcudaInvalidArguments;
+  std::lock_guard<std::mutex> lock(srv->mu);
+  std::vector<double> v = srv->latencies_ms;
+  std::sort(v.begin(), v.end());
+  auto q = [&](double p) {
+    if (v.empty()) return 0.0;
+    const size_t i = std::min(v.size() - 1, static_cast<size_t>(p * (v.size() - 1) + 0.5));
+    return v[i];
+  };
+  if (completed) *completed = v.size();
+  if (p50_ms) *p50_ms = q(0.50);
+  if (p99_ms) *p99_ms = q(0.99);
+  if (p999_ms) *p999_ms = q(0.999);
+  const double secs = std::chrono::duration<double>(Clock::now() - srv->stats_since).count();
+  if (evals_per_s) *evals_per_s = secs > 0 ? static_cast<double>(srv->evals_done) / secs : 0.0;
+  if (reset) {
+    srv->latencies_ms.clear();
+    srv->evals_done = 0;
+    srv->stats_since = Clock::now();
+  }
+  return mhcudaSuccess;
+}
+
+enum MHCUDAResult mhcuda_server_stop(MinhashCudaServer *srv) {
+  delete srv;
+  return mhcudaSuccess;
+}
+
+}  // extern "C"

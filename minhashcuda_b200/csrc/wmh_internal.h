@@ -102,5 +102,7 @@ struct GeneratorView {
   cudaStream_t stream;
 };
 bool generator_view(const MinhashCudaGenerator_ *gen, GeneratorView *view);
+// The engine's work decomposition for `nnz` entries in `rows` rows.
+HashPlan plan_for_generator(const MinhashCudaGenerator_ *gen, uint64_t nnz, uint64_t rows);
 
 }  // namespace mhb
