@@ -283,6 +283,185 @@ def run_batched(args, rank, world, local):
         print(json.dumps(line), flush=True)
 
 
+def run_serving(args, rank, world, local):
+    """Serving: Poisson-arriving requests over three resident generators
+    (2^20 dims / 128 samples, 2^22 / 64, 2^24 / 256; 1.6 + 3.2 + 51.5 GB of
+    parameters), each request a CSR of log-uniform 1..50,000 rows with
+    Zipf-tailed row nnz (median 100), through the continuous-batching server.
+    First the saturated throughput ("batched peak"), then p50/p99/p99.9
+    latency and throughput at fractions of it.  Request buffers are
+    page-locked."""
+    import threading
+    import torch
+    import minhashcuda_b200 as mb
+    from minhashcuda_b200 import synth
+    from minhashcuda_b200.server import Server
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    lib = mb.capi()
+    specs = [synth.WORKLOADS[k] for k in ("serving_g1", "serving_g2", "serving_g3")]
+    gens, pools = [], []
+    t0 = time.perf_counter()
+    for w in specs:
+        st = ctypes.c_int(-1)
+        g = lib.mhcuda_init(w.dim, w.samples, w.seed, 0, 1 << local, 0, ctypes.byref(st))
+        assert g, f"mhcuda_init({w.dim}, {w.samples}) failed: {st.value}"
+        ip, cols, wts = synth.host_csr(w, 0, w.rows)
+
+        def pin(a):
+            t = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True)
+            v = t.numpy().view(a.dtype)[:a.size]
+            v[...] = a
+            return v, t
+
+        (pw, tw), (pc, tc), (pi, ti) = pin(wts), pin(cols), pin(ip)
+        gens.append(g)
+        pools.append({"w": pw, "c": pc, "ip": pi, "keep": (tw, tc, ti), "S": w.samples,
+                      "rows": w.rows})
+        del ip, cols, wts
+    log(f"serving: generators and pools ready in {time.perf_counter() - t0:.1f}s")
+    rng = np.random.default_rng(4)
+    max_rows = 50000
+
+    def make_req():
+        gi = int(rng.integers(0, 3))
+        p = pools[gi]
+        rows = int(min(max_rows, max(1, np.floor(np.exp(rng.uniform(0, np.log(max_rows)))))))
+        r0 = int(rng.integers(0, p["rows"] - rows + 1))
+        nnz = int(p["ip"][r0 + rows]) - int(p["ip"][r0])
+        return gi, r0, rows, nnz * p["S"]
+
+    # Page-locked output rings per generator (recycled once a request is waited for).
+    ring = 48
+    outs = []
+    for p in pools:
+        t = torch.empty((ring, max_rows, p["S"], 2), dtype=torch.int32, pin_memory=True)
+        outs.append((t, t.numpy().view(np.uint32)))
+    free = [list(range(ring)) for _ in pools]
+    free_cv = threading.Condition()
+
+    srv = Server(hbm_budget=args.serving_budget << 30, lanes=args.serving_lanes,
+                 devices=1 << local)
+
+    def submit(req):
+        gi, r0, rows, _ = req
+        p = pools[gi]
+        with free_cv:
+            while not free[gi]:
+                free_cv.wait()
+            slot = free[gi].pop()
+        out = outs[gi][1][slot][:rows]
+        t = srv.submit_raw(gens[gi], p["w"], p["c"], p["ip"][r0:r0 + rows + 1], rows, out)
+        return t, gi, slot
+
+    def release(gi, slot):
+        with free_cv:
+            free[gi].append(slot)
+            free_cv.notify()
+
+    def run_closed(reqs):
+        """Submits back to back; when a generator's output ring is empty the
+        oldest outstanding request is waited for first (bounded window)."""
+        import collections
+        t = time.perf_counter()
+        pend = collections.deque()
+        for r in reqs:
+            while not free[r[0]]:
+                tk, g2, slot = pend.popleft()
+                srv.wait(tk, timeout=120.0)
+                release(g2, slot)
+            pend.append(submit(r))
+        while pend:
+            tk, g2, slot = pend.popleft()
+            srv.wait(tk, timeout=120.0)
+            release(g2, slot)
+        return time.perf_counter() - t
+
+    run_closed([make_req() for _ in range(60)])  # warm-up
+    peak_reqs = [make_req() for _ in range(400)]
+    peak_t = run_closed(peak_reqs)
+    peak = sum(r[3] for r in peak_reqs) / peak_t
+    mean_evals = float(np.mean([make_req()[3] for _ in range(20000)]))
+    log(f"serving: saturated throughput {peak:.3e} evals/s over 400 requests")
+
+    levels = []
+    for frac in args.serving_loads:
+        lam = frac * peak / mean_evals
+        duration = args.serving_seconds
+        arrivals = np.cumsum(rng.exponential(1.0 / lam, int(lam * duration * 1.2) + 10))
+        arrivals = arrivals[arrivals < duration]
+        reqs = [make_req() for _ in arrivals]
+        lat = []
+        done_evals = [0]
+        q = []
+        qcv = threading.Condition()
+
+        def waiter():
+            n = 0
+            while n < len(reqs):
+                with qcv:
+                    while not q:
+                        qcv.wait()
+                    tk, gi, slot, ev = q.pop(0)
+                _, ms = srv.wait(tk, timeout=120.0, with_latency=True)
+                release(gi, slot)
+                lat.append(ms)
+                done_evals[0] += ev
+                n += 1
+
+        th = threading.Thread(target=waiter)
+        th.start()
+        start = time.perf_counter()
+        for at, r in zip(arrivals, reqs):
+            delay = start + at - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            tk, gi, slot = submit(r)
+            with qcv:
+                q.append((tk, gi, slot, r[3]))
+                qcv.notify()
+        th.join()
+        elapsed = time.perf_counter() - start
+        a = np.sort(np.array(lat))
+        levels.append({"load": frac, "offered_evals_per_s": lam * mean_evals,
+                       "requests": len(reqs), "evals_per_s": done_evals[0] / elapsed,
+                       "p50_ms": float(np.percentile(a, 50)), "p99_ms": float(np.percentile(a, 99)),
+                       "p999_ms": float(np.percentile(a, 99.9)), "max_ms": float(a[-1])})
+        log(f"serving: load {frac:.2f}: {levels[-1]}")
+
+    # Each served result equals the same request hashed alone.
+    exact = True
+    for r in [make_req() for _ in range(12)]:
+        gi, r0, rows, _ = r
+        p = pools[gi]
+        tk, g2, slot = submit(r)
+        srv.wait(tk, timeout=120.0)
+        served = outs[gi][1][slot][:rows].copy()
+        release(g2, slot)
+        alone = np.empty_like(served)
+        assert lib.mhcuda_calc(gens[gi], p["w"].ctypes.data, p["c"].ctypes.data,
+                               p["ip"][r0:].ctypes.data, rows, alone.ctypes.data) == 0
+        exact &= bool(np.array_equal(served, alone))
+    srv.stop()
+    for g in gens:
+        lib.mhcuda_fini(g)
+    at80 = min(levels, key=lambda l: abs(l["load"] - 0.8))
+    line = {
+        "metric": "WMH serving p99 latency at 80% of saturated throughput (3 resident generators)",
+        "value": at80["p99_ms"], "unit": "ms", "n_gpus": 1, "steps": len(levels), "warmup": 1,
+        "ms_per_step": None, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded, generated on the device, page-locked host pools)",
+        "config": {"workload": "serving: generators 2^20/128, 2^22/64, 2^24/256; requests of "
+                               "log-uniform 1..50000 rows, row nnz 50*(1+Zipf(2)), Poisson arrivals",
+                   "lanes": args.serving_lanes, "hbm_budget_gib": args.serving_budget,
+                   "seconds_per_level": args.serving_seconds},
+        "saturated_evals_per_s": peak, "mean_evals_per_request": mean_evals, "levels": levels,
+        "bit_exact_served_vs_alone": exact,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def workload_config(w, args):
     return {"workload": f"{w.name}: {w.rows} rows x {w.dim} dims, samples {w.samples}, "
                         f"row nnz {['Poisson', 'lognormal', 'log-uniform', 'Zipf'][w.nnz_kind]}"
@@ -298,7 +477,11 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="large", choices=["large", "batched"])
+    ap.add_argument("--workload", default="large", choices=["large", "batched", "serving"])
+    ap.add_argument("--serving-budget", type=int, default=24, help="server HBM budget, GiB")
+    ap.add_argument("--serving-lanes", type=int, default=4)
+    ap.add_argument("--serving-seconds", type=float, default=6.0)
+    ap.add_argument("--serving-loads", type=float, nargs="+", default=[0.5, 0.8, 0.9])
     ap.add_argument("--rows", type=int, default=0, help="override the row count (smaller runs)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -310,6 +493,8 @@ def main():
         return run_reference_arm(args, rank)
     if args.workload == "batched":
         return run_batched(args, rank, world, local)
+    if args.workload == "serving":
+        return run_serving(args, rank, world, local)
 
     import torch
     import minhashcuda_b200 as mb

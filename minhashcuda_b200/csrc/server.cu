@@ -50,6 +50,8 @@ struct Request {
   uint32_t *output = nullptr;
   Clock::time_point submitted, finished;
   uint32_t units_left = 0;
+  bool in_pinned = false;   // weights and cols are page-locked: large units copy directly
+  bool out_pinned = false;  // output is page-locked: large units copy hashes directly
   MHCUDAResult result = mhcudaSuccess;
   bool cancelled = false;
   bool done = false;
@@ -73,6 +75,7 @@ struct Lane {
   uint32_t *hc = nullptr, *hip = nullptr, *hout = nullptr, *hstatus = nullptr;
   std::vector<Unit> units;
   std::vector<uint64_t> unit_rows;  // row offset of each unit inside the batch
+  std::vector<uint8_t> unit_direct; // hashes already copied straight to the caller
   bool busy = false;
 };
 
@@ -125,6 +128,19 @@ void CUDART_CB notify_worker(void *p) {
   srv->signals.fetch_add(1);
   srv->wake.notify_one();
 }
+
+bool is_pinned(const void *p) {
+  cudaPointerAttributes attr{};
+  if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return attr.type == cudaMemoryTypeHost;
+}
+
+// Units at least this large move between page-locked caller memory and the
+// device with their own copies instead of through the lane's staging.
+constexpr size_t kDirectCopyBytes = static_cast<size_t>(1) << 20;
 
 void par_copy(void *dst, const void *src, size_t bytes) {
   const size_t kSplit = static_cast<size_t>(16) << 20;
@@ -189,17 +205,42 @@ MHCUDAResult MinhashCudaServer_::run_units(Lane &lane, const std::vector<Unit> &
     lane.unit_rows[k + 1] = R;
     pos[k + 1] = N;
   }
+  const cudaStream_t st = lane.stream;
+  cudaError_t e = cudaSuccess;
+  // Staged units are gathered into contiguous runs of the staging buffers;
+  // each run goes over in one copy.  Large page-locked units copy directly.
+  uint64_t run_begin = 0, run_end = 0;
+  auto flush_run = [&]() {
+    if (run_end > run_begin && e == cudaSuccess) {
+      e = cudaMemcpyAsync(lane.w + run_begin, lane.hw + run_begin, (run_end - run_begin) * 4,
+                          cudaMemcpyHostToDevice, st);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(lane.c + run_begin, lane.hc + run_begin, (run_end - run_begin) * 4,
+                            cudaMemcpyHostToDevice, st);
+    }
+    run_begin = run_end;
+  };
   for (size_t k = 0; k < units.size(); ++k) {
     const Unit &u = units[k];
     const uint32_t b = u.req->rows[u.r0];
     const uint64_t n = pos[k + 1] - pos[k];
-    par_copy(lane.hw + pos[k], u.req->weights + b, n * 4);
-    par_copy(lane.hc + pos[k], u.req->cols + b, n * 4);
+    if (u.req->in_pinned && n * 4 >= kDirectCopyBytes) {
+      flush_run();
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(lane.w + pos[k], u.req->weights + b, n * 4, cudaMemcpyHostToDevice, st);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(lane.c + pos[k], u.req->cols + b, n * 4, cudaMemcpyHostToDevice, st);
+      run_begin = run_end = pos[k + 1];
+    } else {
+      par_copy(lane.hw + pos[k], u.req->weights + b, n * 4);
+      par_copy(lane.hc + pos[k], u.req->cols + b, n * 4);
+      run_end = pos[k + 1];
+    }
     uint32_t *ip = lane.hip + lane.unit_rows[k];
     for (uint32_t x = u.r0; x < u.r1; ++x) ip[x - u.r0] = static_cast<uint32_t>(pos[k] + (u.req->rows[x] - b));
   }
+  flush_run();
   lane.hip[R] = static_cast<uint32_t>(N);
-  const cudaStream_t st = lane.stream;
   const uint32_t s_pad = g.s_pad;
   mhb::HashPlan plan = mhb::plan_for_generator(units.front().req->gen, N, R);
   // Keep the chunk table and partials inside the lane's fixed scratch:
@@ -234,15 +275,26 @@ MHCUDAResult MinhashCudaServer_::run_units(Lane &lane, const std::vector<Unit> &
   a.part_kt = lane.part_kt;
   a.out = lane.out;
   a.status = lane.status;
-  cudaError_t e = cudaMemcpyAsync(lane.ip, lane.hip, (R + 1) * 4, cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess && N) e = cudaMemcpyAsync(lane.w, lane.hw, N * 4, cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess && N) e = cudaMemcpyAsync(lane.c, lane.hc, N * 4, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(lane.ip, lane.hip, (R + 1) * 4, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(lane.status, 0, 4, st);
   if (e == cudaSuccess) e = mhb::launch_plan(a, st);
   if (e == cudaSuccess) e = mhb::launch_hash(a, plan, st);
   if (e == cudaSuccess && plan.nchunks > 1) e = mhb::launch_finalize(a, st);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(lane.hout, lane.out, R * g.samples * 8, cudaMemcpyDeviceToHost, st);
+  // Hashes: large units into page-locked outputs directly, the rest through
+  // the lane's staging (copied out by complete()).
+  lane.unit_direct.assign(units.size(), 0);
+  for (size_t k = 0; k < units.size() && e == cudaSuccess; ++k) {
+    const Unit &u = units[k];
+    const size_t bytes = unit_out_bytes(u);
+    const size_t off = lane.unit_rows[k] * g.samples * 2;
+    if (!solo && u.req->out_pinned && bytes >= kDirectCopyBytes) {
+      e = cudaMemcpyAsync(u.req->output + static_cast<size_t>(u.r0) * g.samples * 2, lane.out + off,
+                          bytes, cudaMemcpyDeviceToHost, st);
+      lane.unit_direct[k] = 1;
+    } else {
+      e = cudaMemcpyAsync(lane.hout + off, lane.out + off, bytes, cudaMemcpyDeviceToHost, st);
+    }
+  }
   if (e == cudaSuccess) e = cudaMemcpyAsync(lane.hstatus, lane.status, 4, cudaMemcpyDeviceToHost, st);
   // The event is recorded before the wake-up callback so the worker finds it
   // complete when the callback wakes it.
@@ -330,6 +382,7 @@ void MinhashCudaServer_::complete(Lane &lane) {
   } else {
     for (size_t k = 0; k < units.size(); ++k) {
       const Unit &u = units[k];
+      if (lane.unit_direct[k]) continue;
       par_copy(u.req->output + static_cast<size_t>(u.r0) * u.req->g.samples * 2,
                lane.hout + lane.unit_rows[k] * u.req->g.samples * 2, unit_out_bytes(u));
     }
@@ -500,6 +553,8 @@ enum MHCUDAResult mhcuda_server_submit(MinhashCudaServer *srv, const MinhashCuda
     if ((static_cast<size_t>(rows[i + 1]) - rows[i]) * 8 + 8 > srv->in_cap)
       return mhcudaMemoryAllocationFailure;
   }
+  r->in_pinned = is_pinned(weights) && is_pinned(cols);
+  r->out_pinned = is_pinned(output);
   r->gen = gen;
   r->weights = weights;
   r->cols = cols;

@@ -17,6 +17,10 @@ The shapes follow the benchmark configurations of the reference's workload
   batched   4096 matrices x 2^20 dims, rows log-uniform in [1, 4096], row nnz
             lognormal(median 64, sigma 1.5) clipped to [1, 20000], uniform
             columns, lognormal values, samples 256
+  serving   three resident generators (2^20 dims / 128 samples, 2^22 / 64,
+            2^24 / 256), each with a pool of 400,000 rows whose nnz is
+            50 * (1 + K), P(K >= k) = 1/k (median 100, capped at 50,000);
+            requests are row ranges of log-uniform length in [1, 50,000]
 """
 from __future__ import annotations
 
@@ -55,6 +59,12 @@ WORKLOADS = {
     "streamed": Workload("streamed", rows=10_000_000, dim=12_000_000, samples=128, seed=1000,
                          nnz_kind=NNZ_LOGNORMAL, nnz_p1=200.0, nnz_p2=1.354, nnz_lo=1,
                          nnz_hi=50000, extra={"block_rows": 524_288}),
+    "serving_g1": Workload("serving_g1", rows=400_000, dim=1 << 20, samples=128, seed=41,
+                           nnz_kind=NNZ_ZIPF, nnz_p1=50.0, nnz_p2=2.0, nnz_lo=1, nnz_hi=50000),
+    "serving_g2": Workload("serving_g2", rows=400_000, dim=1 << 22, samples=64, seed=42,
+                           nnz_kind=NNZ_ZIPF, nnz_p1=50.0, nnz_p2=2.0, nnz_lo=1, nnz_hi=50000),
+    "serving_g3": Workload("serving_g3", rows=400_000, dim=1 << 24, samples=256, seed=43,
+                           nnz_kind=NNZ_ZIPF, nnz_p1=50.0, nnz_p2=2.0, nnz_lo=1, nnz_hi=50000),
     "batched": Workload("batched", rows=0, dim=1 << 20, samples=256, seed=3,
                         nnz_kind=NNZ_LOGNORMAL, nnz_p1=64.0, nnz_p2=1.5, nnz_lo=1,
                         nnz_hi=20000, extra={"matrices": 4096, "max_rows": 4096}),

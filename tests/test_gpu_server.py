@@ -137,3 +137,39 @@ def test_cancel_and_refusals():
             assert srv.wait(srv.submit(g, huge)).shape == (1, 256, 2)
     finally:
         _fini(gens)
+
+
+def test_page_locked_requests_copy_directly():
+    """Large requests in page-locked memory bypass the lane staging; results
+    still equal mhcuda_calc alone."""
+    import torch
+    from minhashcuda_b200 import libMHCUDA as L
+    from minhashcuda_b200.server import Server
+    rng = np.random.default_rng(9)
+    gens = _gens([(50000, 128)], rng)
+    g = gens[0][0]
+
+    def pinned(a):
+        t = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True)
+        v = t.numpy().view(a.dtype)[:a.size].reshape(a.shape)
+        v[...] = a
+        return v, t
+
+    try:
+        mats = [random_csr(rng, int(rng.integers(1000, 4000)), 50000, 400) for _ in range(6)]
+        keep = []
+        with Server(hbm_budget=2 << 30, lanes=2) as srv:
+            tickets = []
+            for m in mats:
+                d, t1 = pinned(m.data.astype(np.float32))
+                i, t2 = pinned(m.indices.astype(np.uint32))
+                p, t3 = pinned(m.indptr.astype(np.uint32))
+                o, t4 = pinned(np.zeros((m.shape[0], 128, 2), np.uint32))
+                keep += [t1, t2, t3, t4]
+                tickets.append(srv.submit_raw(g, d, i, p, m.shape[0], o))
+            outs = [srv.wait(t) for t in tickets]
+        for m, out in zip(mats, outs):
+            np.testing.assert_array_equal(out, L.minhash_cuda_calc(g, m))
+        del keep
+    finally:
+        _fini(gens)
