@@ -479,7 +479,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="large", choices=["large", "batched", "serving"])
     ap.add_argument("--serving-budget", type=int, default=24, help="server HBM budget, GiB")
-    ap.add_argument("--serving-lanes", type=int, default=4)
+    ap.add_argument("--serving-lanes", type=int, default=8)
     ap.add_argument("--serving-seconds", type=float, default=6.0)
     ap.add_argument("--serving-loads", type=float, nargs="+", default=[0.5, 0.8, 0.9])
     ap.add_argument("--rows", type=int, default=0, help="override the row count (smaller runs)")

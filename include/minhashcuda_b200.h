@@ -133,7 +133,8 @@ enum MHCUDAResult mhcuda_server_wait(MinhashCudaServer *srv, uint64_t ticket, do
                                      double *latency_ms);
 
 /* Drops the request's blocks that have not started; it then completes with
- * mhcudaRuntimeError. */
+ * mhcudaRuntimeError.  Returns mhcudaInvalidArguments for an unknown ticket or
+ * a request that has already finished (its result stands). */
 enum MHCUDAResult mhcuda_server_cancel(MinhashCudaServer *srv, uint64_t ticket);
 
 /* Latency percentiles over completed requests and hashed nnz*samples per

@@ -1,17 +1,20 @@
 // Continuous-batching hash server (mhcuda_server_*).
 //
 // The reference has no server: every mhcuda_calc call is one synchronous
-// launch per device (minhashcuda.cc:583-642).  Here a worker thread keeps
-// several "lanes" busy on one device.  Each lane owns a CUDA stream, device
-// buffers for one batch (CSR in, hashes out, chunk scratch) and pinned host
-// staging.  Requests are cut into row-range units small enough for a lane;
-// whenever a lane is free it takes the oldest pending unit and every
-// following unit of the same generator that still fits, gathers them into
-// one CSR, and runs copy-in, the plan/hash/finalize kernels and copy-out on
-// its stream.  Lanes run concurrently, so a request that arrives while other
-// batches are on the GPU starts as soon as a lane frees up and its work
-// overlaps theirs.  Device memory is bounded by the budget given at start:
-// the lanes are sized from it once and nothing grows afterwards.
+// launch per device (minhashcuda.cc:583-642).  Here several "lanes" share one
+// device.  Each lane is a host thread with its own CUDA stream, device buffers
+// for one batch (CSR in, hashes out, chunk scratch) and pinned host staging.
+// Active requests sit in a round-robin ring.  A free lane walks the ring and
+// takes the next row block ("unit", at most max_unit_evals nnz*samples) of
+// every request of one generator in turn until its batch is full, gathers
+// them into one CSR, runs copy-in, the plan/hash/finalize kernels and
+// copy-out on its stream, waits for its own event and hands the hashes back.
+// Requests that arrive while batches are on the GPU join the ring at once and
+// get their first unit into the next batch any lane forms, so the device is
+// shared between requests (small ones finish quickly, large ones progress
+// block by block) and lanes overlap each other's copies and kernels.  Device
+// memory is bounded by the budget given at start: the lanes are sized from
+// it once and nothing grows afterwards.
 //
 // Per-request guarantees: the hashes equal a lone mhcuda_calc of the same
 // request bit for bit (same kernels, same per-row arithmetic; the batch only
@@ -19,10 +22,10 @@
 // reports invalid CSR is re-run unit by unit so that only the offending
 // request fails.
 #include <algorithm>
-#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <memory>
@@ -49,9 +52,10 @@ struct Request {
   uint32_t length = 0;
   uint32_t *output = nullptr;
   Clock::time_point submitted, finished;
-  uint32_t units_left = 0;
-  bool in_pinned = false;   // weights and cols are page-locked: large units copy directly
-  bool out_pinned = false;  // output is page-locked: large units copy hashes directly
+  uint32_t next_row = 0;        // first row not yet handed to a lane
+  uint32_t inflight = 0;        // units handed out and not yet complete
+  bool in_pinned = false;       // weights and cols are page-locked: large units copy directly
+  bool out_pinned = false;      // output is page-locked: large units copy hashes directly
   MHCUDAResult result = mhcudaSuccess;
   bool cancelled = false;
   bool done = false;
@@ -76,10 +80,17 @@ struct Lane {
   std::vector<Unit> units;
   std::vector<uint64_t> unit_rows;  // row offset of each unit inside the batch
   std::vector<uint8_t> unit_direct; // hashes already copied straight to the caller
-  bool busy = false;
+  std::thread thread;
 };
 
 size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
+
+uint64_t env_u64(const char *name, uint64_t fallback) {
+  const char *v = getenv(name);
+  if (!v || !*v) return fallback;
+  const unsigned long long x = strtoull(v, nullptr, 10);
+  return x ? x : fallback;
+}
 
 }  // namespace
 
@@ -90,28 +101,27 @@ struct MinhashCudaServer_ {
   // Per-lane capacities (bytes).
   size_t in_cap = 0, out_cap = 0, scratch_cap = 0;
   size_t scratch_unit = 0;  // scratch = chunk_row (1 unit) | part_ln (4) | part_kt (8)
+  uint64_t max_unit_evals = 128ull << 20;   // nnz*samples of one row block
+  uint64_t max_batch_evals = 1024ull << 20; // nnz*samples of one lane batch
   std::vector<Lane> lanes;
 
   std::mutex mu;
-  std::condition_variable wake;       // worker: new work or a lane finished
-  std::condition_variable finished;   // waiters: a request completed
-  std::deque<Request *> incoming;     // submitted, not yet cut into units
-  std::deque<Unit> pending;           // units waiting for a lane
+  std::condition_variable work;      // lanes: a request joined the ring (or stop)
+  std::condition_variable finished;  // waiters: a request completed
+  std::deque<Request *> ring;        // requests with rows not yet handed out
   std::unordered_map<uint64_t, std::unique_ptr<Request>> requests;
-  std::vector<double> latencies_ms;   // completed requests, for mhcuda_server_stats
+  std::vector<double> latencies_ms;  // completed requests, for mhcuda_server_stats
   uint64_t next_ticket = 1;
   uint64_t evals_done = 0;
   Clock::time_point stats_since = Clock::now();
   bool stop = false;
-  std::atomic<int> signals{0};
-  std::thread worker;
 
   ~MinhashCudaServer_();
-  void run();
+  void lane_loop(Lane &lane);
   bool take(Lane &lane);
-  void start(Lane &lane);
-  void complete(Lane &lane);
+  void complete(Lane &lane, MHCUDAResult launch_result);
   MHCUDAResult run_units(Lane &lane, const std::vector<Unit> &units, bool solo);
+  void finish_locked(Request *r, Clock::time_point now);
   size_t unit_in_bytes(const Unit &u) const {
     const uint64_t n = static_cast<uint64_t>(u.req->rows[u.r1]) - u.req->rows[u.r0];
     return n * 8 + (static_cast<size_t>(u.r1 - u.r0) + 1) * 4;
@@ -122,12 +132,6 @@ struct MinhashCudaServer_ {
 };
 
 namespace {
-
-void CUDART_CB notify_worker(void *p) {
-  auto *srv = static_cast<MinhashCudaServer_ *>(p);
-  srv->signals.fetch_add(1);
-  srv->wake.notify_one();
-}
 
 bool is_pinned(const void *p) {
   cudaPointerAttributes attr{};
@@ -148,7 +152,7 @@ void par_copy(void *dst, const void *src, size_t bytes) {
     memcpy(dst, src, bytes);
     return;
   }
-  const unsigned n = std::min(8u, std::max(1u, std::thread::hardware_concurrency()));
+  const unsigned n = 4;
   const size_t part = (((bytes + n - 1) / n) + 4095) & ~static_cast<size_t>(4095);
   std::vector<std::thread> pool;
   for (unsigned t = 0; t < n; ++t) {
@@ -169,8 +173,9 @@ MinhashCudaServer_::~MinhashCudaServer_() {
     std::lock_guard<std::mutex> lock(mu);
     stop = true;
   }
-  wake.notify_all();
-  if (worker.joinable()) worker.join();
+  work.notify_all();
+  for (Lane &l : lanes)
+    if (l.thread.joinable()) l.thread.join();
   cudaSetDevice(device);
   for (Lane &l : lanes) {
     if (l.stream) cudaStreamSynchronize(l.stream);
@@ -296,10 +301,7 @@ MHCUDAResult MinhashCudaServer_::run_units(Lane &lane, const std::vector<Unit> &
     }
   }
   if (e == cudaSuccess) e = cudaMemcpyAsync(lane.hstatus, lane.status, 4, cudaMemcpyDeviceToHost, st);
-  // The event is recorded before the wake-up callback so the worker finds it
-  // complete when the callback wakes it.
   if (e == cudaSuccess) e = cudaEventRecord(lane.done_ev, st);
-  if (e == cudaSuccess && !solo) e = cudaLaunchHostFunc(st, notify_worker, this);
   if (e == cudaSuccess && solo) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -308,65 +310,109 @@ MHCUDAResult MinhashCudaServer_::run_units(Lane &lane, const std::vector<Unit> &
   return mhcudaSuccess;
 }
 
-// Under `mu`: moves the oldest pending unit and every later unit of the same
-// generator that still fits the lane (bounded look-ahead keeps admission
-// close to FIFO) into lane.units.  Returns false if nothing was taken.
+// Under `mu`.
+void MinhashCudaServer_::finish_locked(Request *r, Clock::time_point now) {
+  r->done = true;
+  r->finished = now;
+  if (!r->cancelled)
+    latencies_ms.push_back(std::chrono::duration<double, std::milli>(now - r->submitted).count());
+}
+
+// Under `mu`: fills lane.units by walking the ring from its head, one unit
+// per request of the first request's generator per pass, until the batch is
+// full; requests whose rows are all handed out leave the ring, the others
+// rotate to its back (round-robin).  Returns false if nothing was taken.
 bool MinhashCudaServer_::take(Lane &lane) {
   std::vector<Unit> batch;
   size_t in = 0, out = 0;
+  uint64_t evals = 0;
   const MinhashCudaGenerator_ *gen = nullptr;
-  size_t scanned = 0;
-  for (auto it = pending.begin(); it != pending.end() && scanned < 512; ++scanned) {
-    if (it->req->cancelled) {
-      Request *r = it->req;
-      it = pending.erase(it);
-      if (--r->units_left == 0 && !r->done) {
-        r->done = true;
-        r->finished = Clock::now();
-        finished.notify_all();
-      }
-      continue;
-    }
-    if (gen && it->req->gen != gen) {
+  // Small-first: a request whose remaining work fits one unit joins this
+  // batch ahead of the round-robin, so short requests never wait behind the
+  // blocks of long ones.
+  auto remaining = [](const Request *r) {
+    return (static_cast<uint64_t>(r->rows[r->length]) - r->rows[r->next_row]) * r->g.samples;
+  };
+  for (auto it = ring.begin(); it != ring.end();) {
+    Request *r = *it;
+    if (r->cancelled || remaining(r) > max_unit_evals || (gen && r->gen != gen)) {
       ++it;
       continue;
     }
-    const size_t ui = unit_in_bytes(*it), uo = unit_out_bytes(*it);
-    if (!batch.empty() && (in + ui > in_cap || out + uo > out_cap)) break;
-    gen = it->req->gen;
+    const size_t ui = static_cast<size_t>(r->rows[r->length] - r->rows[r->next_row]) * 8 +
+                      (static_cast<size_t>(r->length - r->next_row) + 1) * 4;
+    const size_t uo = static_cast<size_t>(r->length - r->next_row) * r->g.samples * 8;
+    if (in + ui > in_cap || out + uo > out_cap || evals + remaining(r) > max_batch_evals) {
+      ++it;
+      continue;
+    }
+    gen = r->gen;
+    evals += remaining(r);
     in += ui;
     out += uo;
-    batch.push_back(*it);
-    it = pending.erase(it);
+    batch.push_back(Unit{r, r->next_row, r->length});
+    r->next_row = r->length;
+    ++r->inflight;
+    it = ring.erase(it);
+  }
+  bool grew = true;
+  while (grew && !ring.empty()) {
+    grew = false;
+    const size_t n = ring.size();
+    for (size_t k = 0; k < n && !ring.empty(); ++k) {
+      Request *r = ring.front();
+      ring.pop_front();
+      if (r->cancelled) {
+        if (r->inflight == 0 && !r->done) finish_locked(r, Clock::now());
+        continue;
+      }
+      if ((gen && r->gen != gen) || evals >= max_batch_evals) {
+        ring.push_back(r);
+        continue;
+      }
+      // Next row block of r: at least one row, then rows while the unit stays
+      // under max_unit_evals and the batch under the lane's capacities.
+      const uint64_t S = r->g.samples;
+      const size_t row_out = S * 8;
+      uint32_t r1 = r->next_row;
+      uint64_t ue = 0;
+      size_t ui = 4, uo = 0;
+      while (r1 < r->length) {
+        const uint64_t nz = static_cast<uint64_t>(r->rows[r1 + 1]) - r->rows[r1];
+        const size_t add_in = nz * 8 + 4;
+        const bool first = r1 == r->next_row;
+        if (in + ui + add_in > in_cap || out + uo + row_out > out_cap) break;
+        if (!first && (ue + nz * S > max_unit_evals || evals + ue + nz * S > max_batch_evals))
+          break;
+        ui += add_in;
+        uo += row_out;
+        ue += nz * S;
+        ++r1;
+      }
+      if (r1 == r->next_row) {  // does not fit what is left of this batch
+        ring.push_back(r);
+        continue;
+      }
+      gen = r->gen;
+      batch.push_back(Unit{r, r->next_row, r1});
+      r->next_row = r1;
+      ++r->inflight;
+      in += ui;
+      out += uo;
+      evals += ue;
+      grew = true;
+      if (r->next_row < r->length) ring.push_back(r);
+    }
   }
   if (batch.empty()) return false;
   lane.units = std::move(batch);
-  lane.busy = true;
   return true;
 }
 
-// Without `mu`: gathers and enqueues the lane's batch.
-void MinhashCudaServer_::start(Lane &lane) {
-  const MHCUDAResult r = run_units(lane, lane.units, false);
-  if (r == mhcudaSuccess) return;
-  std::lock_guard<std::mutex> lock(mu);
-  const Clock::time_point now = Clock::now();
-  for (const Unit &u : lane.units) {
-    u.req->result = r;
-    if (--u.req->units_left == 0) {
-      u.req->done = true;
-      u.req->finished = now;
-    }
-  }
-  lane.units.clear();
-  lane.busy = false;
-  finished.notify_all();
-}
-
-void MinhashCudaServer_::complete(Lane &lane) {
+void MinhashCudaServer_::complete(Lane &lane, MHCUDAResult launch_result) {
   std::vector<Unit> units = std::move(lane.units);
-  std::vector<MHCUDAResult> unit_result(units.size(), mhcudaSuccess);
-  if (*lane.hstatus != 0) {
+  std::vector<MHCUDAResult> unit_result(units.size(), launch_result);
+  if (launch_result == mhcudaSuccess && *lane.hstatus != 0) {
     // Attribute the invalid input: run every unit of the batch on its own.
     for (size_t k = 0; k < units.size(); ++k) {
       std::vector<Unit> one{units[k]};
@@ -379,7 +425,7 @@ void MinhashCudaServer_::complete(Lane &lane) {
                  unit_out_bytes(u));
       }
     }
-  } else {
+  } else if (launch_result == mhcudaSuccess) {
     for (size_t k = 0; k < units.size(); ++k) {
       const Unit &u = units[k];
       if (lane.unit_direct[k]) continue;
@@ -387,79 +433,34 @@ void MinhashCudaServer_::complete(Lane &lane) {
                lane.hout + lane.unit_rows[k] * u.req->g.samples * 2, unit_out_bytes(u));
     }
   }
-  lane.busy = false;
   std::lock_guard<std::mutex> lock(mu);
   const Clock::time_point now = Clock::now();
   for (size_t k = 0; k < units.size(); ++k) {
     Request *r = units[k].req;
     evals_done += (static_cast<uint64_t>(r->rows[units[k].r1]) - r->rows[units[k].r0]) * r->g.samples;
     if (unit_result[k] != mhcudaSuccess) r->result = unit_result[k];
-    if (--r->units_left == 0) {
-      r->done = true;
-      r->finished = now;
-      if (!r->cancelled)
-        latencies_ms.push_back(std::chrono::duration<double, std::milli>(now - r->submitted).count());
-    }
+    --r->inflight;
+    if (r->inflight == 0 && (r->next_row == r->length || r->cancelled) && !r->done)
+      finish_locked(r, now);
   }
   finished.notify_all();
 }
 
-void MinhashCudaServer_::run() {
+void MinhashCudaServer_::lane_loop(Lane &lane) {
   cudaSetDevice(device);
-  const size_t max_rows_unit = 1u << 20;
   for (;;) {
     {
       std::unique_lock<std::mutex> lock(mu);
-      // Cut new requests into units that fit a lane.
-      while (!incoming.empty()) {
-        Request *r = incoming.front();
-        incoming.pop_front();
-        const size_t row_out = static_cast<size_t>(r->g.samples) * 8;
-        uint32_t r0 = 0;
-        while (r0 < r->length) {
-          uint32_t r1 = r0;
-          size_t in = 4, outb = 0;
-          while (r1 < r->length) {
-            const size_t add_in = (static_cast<size_t>(r->rows[r1 + 1]) - r->rows[r1]) * 8 + 4;
-            if (r1 > r0 && (in + add_in > in_cap || outb + row_out > out_cap ||
-                            r1 - r0 >= max_rows_unit))
-              break;
-            in += add_in;
-            outb += row_out;
-            ++r1;
-          }
-          pending.push_back(Unit{r, r0, r1});
-          ++r->units_left;
-          r0 = r1;
-        }
-      }
-      bool any_busy = false;
-      for (const Lane &l : lanes) any_busy |= l.busy;
-      if (stop && !any_busy && pending.empty()) break;
+      work.wait(lock, [&] { return stop || !ring.empty(); });
+      if (ring.empty()) return;  // stop requested and nothing left
+      if (!take(lane)) continue;
     }
-    bool progressed = false;
-    for (Lane &l : lanes) {
-      if (l.busy && cudaEventQuery(l.done_ev) == cudaSuccess) {
-        complete(l);
-        progressed = true;
-      }
+    MHCUDAResult r = run_units(lane, lane.units, false);
+    if (r == mhcudaSuccess && cudaEventSynchronize(lane.done_ev) != cudaSuccess) {
+      cudaGetLastError();
+      r = mhcudaRuntimeError;
     }
-    std::vector<Lane *> taken;
-    {
-      std::lock_guard<std::mutex> lock(mu);
-      for (Lane &l : lanes)
-        if (!l.busy && !pending.empty() && take(l)) taken.push_back(&l);
-    }
-    for (Lane *l : taken) start(*l);
-    progressed |= !taken.empty();
-    {
-      std::unique_lock<std::mutex> lock(mu);
-      if (!progressed && incoming.empty()) {
-        const int seen = signals.load();
-        wake.wait_for(lock, std::chrono::microseconds(200),
-                      [&] { return stop || !incoming.empty() || signals.load() != seen; });
-      }
-    }
+    complete(lane, r);
   }
 }
 
@@ -492,6 +493,8 @@ MinhashCudaServer *mhcuda_server_start(uint32_t devices, uint64_t hbm_budget_byt
   std::unique_ptr<MinhashCudaServer_> srv(new MinhashCudaServer_());
   srv->device = dev;
   srv->verbosity = verbosity;
+  srv->max_unit_evals = env_u64("MHCUDA_B200_SERVER_UNIT_EVALS", srv->max_unit_evals);
+  srv->max_batch_evals = env_u64("MHCUDA_B200_SERVER_BATCH_EVALS", srv->max_batch_evals);
   cudaDeviceGetAttribute(&srv->sm_count, cudaDevAttrMultiProcessorCount, dev);
   const size_t per_lane = hbm_budget_bytes / lanes;
   srv->in_cap = align256(per_lane * 4 / 10);
@@ -522,14 +525,15 @@ MinhashCudaServer *mhcuda_server_start(uint32_t devices, uint64_t hbm_budget_byt
       set(mhcudaMemoryAllocationFailure);
       return nullptr;
     }
-    // Layout within scratch is decided per batch from s_pad; keep the three
-    // pointers at fixed fractions: chunk_row | part_ln | part_kt (1 : 4 : 8).
     const size_t unit = srv->scratch_unit;
     l.chunk_row = reinterpret_cast<uint32_t *>(scratch);
     l.part_ln = reinterpret_cast<float *>(scratch + unit);
     l.part_kt = reinterpret_cast<uint2 *>(scratch + 5 * unit);
   }
-  srv->worker = std::thread([s = srv.get()]() { s->run(); });
+  for (Lane &l : srv->lanes) {
+    MinhashCudaServer_ *s = srv.get();
+    l.thread = std::thread([s, &l]() { s->lane_loop(l); });
+  }
   set(mhcudaSuccess);
   return srv.release();
 }
@@ -567,10 +571,10 @@ enum MHCUDAResult mhcuda_server_submit(MinhashCudaServer *srv, const MinhashCuda
     if (srv->stop) return mhcudaRuntimeError;
     r->ticket = srv->next_ticket++;
     *ticket = r->ticket;
-    srv->incoming.push_back(r.get());
+    srv->ring.push_back(r.get());
     srv->requests.emplace(r->ticket, std::move(r));
   }
-  srv->wake.notify_one();
+  srv->work.notify_one();
   return mhcudaSuccess;
 }
 
@@ -612,16 +616,12 @@ enum MHCUDAResult mhcuda_server_cancel(MinhashCudaServer *srv, uint64_t ticket) 
   if (r->done) return mhcudaInvalidArguments;
   r->cancelled = true;
   r->result = mhcudaRuntimeError;  // its hashes are not (all) computed
-  // Still in the incoming queue: drop it now.
-  auto q = std::find(srv->incoming.begin(), srv->incoming.end(), r);
-  if (q != srv->incoming.end()) {
-    srv->incoming.erase(q);
-    r->done = true;
-    r->result = mhcudaRuntimeError;
-    r->finished = Clock::now();
+  if (r->inflight == 0) {
+    auto q = std::find(srv->ring.begin(), srv->ring.end(), r);
+    if (q != srv->ring.end()) srv->ring.erase(q);
+    srv->finish_locked(r, Clock::now());
     srv->finished.notify_all();
   }
-  srv->wake.notify_one();
   return mhcudaSuccess;
 }
 

@@ -62,8 +62,10 @@ class Server:
         out = keep[3] if keep else None
         return (out, lat.value) if with_latency else out
 
-    def cancel(self, ticket: int) -> None:
-        check("mhcuda_server_cancel", self._lib.mhcuda_server_cancel(self._h, ticket))
+    def cancel(self, ticket: int) -> bool:
+        """True if the request was cancelled (wait() then raises), False if it
+        had already finished (wait() returns its hashes)."""
+        return self._lib.mhcuda_server_cancel(self._h, ticket) == 0
 
     def stats(self, reset: bool = False) -> dict:
         n = ctypes.c_uint64(0)

@@ -120,21 +120,43 @@ def test_cancel_and_refusals():
             with pytest.raises(mb.MHCUDAError) as e:
                 srv.submit(g, wide)
             assert e.value.code == mb.MEMORY_ALLOCATION_FAILURE
-            # cancel requests while the lanes are busy with earlier ones
+            # cancel requests while the lanes are busy with earlier ones; a
+            # request that already finished reports that and keeps its result
             many = [random_csr(rng, 300, 20000, 200) for _ in range(40)]
             tickets = [srv.submit(g, m) for m in many]
-            cancelled = tickets[-10:]
-            for t in cancelled:
-                srv.cancel(t)
+            cancelled = [t for t in tickets[-10:] if srv.cancel(t)]
             ok = 0
             for t in tickets:
                 try:
                     srv.wait(t)
                     ok += 1
+                    assert t not in cancelled
                 except mb.MHCUDAError as err:
                     assert t in cancelled and err.code == mb.RUNTIME_ERROR
-            assert ok >= 30
+            assert ok == len(tickets) - len(cancelled)
             assert srv.wait(srv.submit(g, huge)).shape == (1, 256, 2)
+    finally:
+        _fini(gens)
+
+
+def test_cancel_pending_request():
+    """With one lane busy on large requests, the last ones are still waiting
+    and are cancelled before any of their rows run."""
+    import minhashcuda_b200 as mb
+    from minhashcuda_b200.server import Server
+    rng = np.random.default_rng(10)
+    gens = _gens([(20000, 256)], rng)
+    g = gens[0][0]
+    try:
+        with Server(hbm_budget=256 << 20, lanes=1) as srv:
+            big = [random_csr(rng, 3000, 20000, 1500) for _ in range(6)]
+            tickets = [srv.submit(g, m) for m in big]
+            assert srv.cancel(tickets[-1])
+            with pytest.raises(mb.MHCUDAError) as e:
+                srv.wait(tickets[-1])
+            assert e.value.code == mb.RUNTIME_ERROR
+            for t in tickets[:-1]:
+                assert srv.wait(t).shape == (3000, 256, 2)
     finally:
         _fini(gens)
 
