@@ -589,6 +589,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-rows", type=int, default=3000)
+    ap.add_argument("--autotune", action="store_true",
+                    help="pick the hash kernel variant with mhcuda_autotune before timing")
     args = ap.parse_args()
 
     rank, world, local = dist_setup()
@@ -650,6 +652,18 @@ def main():
         t = torch.tensor([x], dtype=torch.float64, device="cuda")
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         return float(t.item())
+
+    tuned = None
+    if args.autotune:
+        choice = (ctypes.c_uint32 * 3)()
+        best = ctypes.c_double(0)
+        t_tune = time.perf_counter()
+        assert lib.mhcuda_autotune(gen, weights.data_ptr(), cols.data_ptr(), indptr.data_ptr(),
+                                   R, nnz, out.data_ptr(), sptr, choice, ctypes.byref(best)) == 0
+        tuned = {"samples_per_lane": choice[0], "min_blocks_per_sm": choice[1],
+                 "items_per_resident_warp": choice[2], "best_ms": best.value,
+                 "tuning_s": time.perf_counter() - t_tune}
+        log(f"[rank {rank}] autotune: {tuned}")
 
     # ---- value: device-resident throughput ---------------------------------
     for _ in range(args.warmup):
@@ -759,7 +773,7 @@ def main():
             "config": workload_config(w, args), "rows_per_s": R * world / (ms_step / 1e3),
             "nnz": nnz, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "parity": parity, "clocks": clocks,
-            "gpu_launches": 3 * args.steps,
+            "gpu_launches": 3 * args.steps, "autotuned": tuned,
         }
         print(json.dumps(line), flush=True)
     if pg:

@@ -31,6 +31,21 @@ enum MHCUDAResult mhcuda_calc_device(
     const uint32_t *d_cols, const uint32_t *d_rows, uint32_t length,
     uint32_t nnz, uint32_t *d_output, void *stream);
 
+/* Autotuner: times the hash kernel's variants (samples per lane 1/2/4,
+ * register budget, chunk granularity) on this device-resident CSR (same
+ * arguments as mhcuda_calc_device; d_output receives the hashes), keeps the
+ * fastest for launches of the same shape class (log2 of nnz and of the mean
+ * row length) on this generator, and returns it in choice[3] = {samples per
+ * lane, min blocks per SM, items per resident warp} and its time in *best_ms
+ * (either may be NULL).  Results never depend on the choice.  Waits for
+ * completion.  No counterpart in the reference (its launch shape is fixed by
+ * host binpacking, minhashcuda.cc:457-528, and kernel.cu:155-160). */
+enum MHCUDAResult mhcuda_autotune(
+    const MinhashCudaGenerator *gen, const float *d_weights,
+    const uint32_t *d_cols, const uint32_t *d_rows, uint32_t length,
+    uint32_t nnz, uint32_t *d_output, void *stream, uint32_t *choice,
+    double *best_ms);
+
 /* Waits for the generator's device work and returns mhcudaInvalidArguments
  * if a preceding mhcuda_calc_device saw invalid CSR content (and clears the
  * flag), mhcudaRuntimeError on a CUDA error, else mhcudaSuccess.

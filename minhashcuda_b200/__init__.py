@@ -63,6 +63,8 @@ SIGNATURES = {
     "mhcuda_fini": (_RES, [_P]),
     "mhcuda_calc_device": (_RES, [_P, _P, _P, _P, _U32, _U32, _P, _P]),
     "mhcuda_device_status": (_RES, [_P]),
+    "mhcuda_autotune": (_RES, [_P, _P, _P, _P, _U32, _U32, _P, _P,
+                               ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_double)]),
     "mhcuda_calc_device_noalloc": (_RES, [_P, _P, _P, _P, _U32, _U32, _P, _P]),
     "mhcuda_calc_batch": (_RES, [_P, _U32, _P, _P, _P, _P, _P]),
     "mhcuda_debug_device_logf": (_RES, [_U32, _P, _P, ctypes.c_uint64]),

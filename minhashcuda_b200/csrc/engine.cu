@@ -20,6 +20,7 @@
 #include <memory>
 #include <mutex>
 #include <thread>
+#include <unordered_map>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -114,6 +115,21 @@ int env_int(const char *name, int fallback) {
   return atoi(v);
 }
 
+// A hash-kernel configuration chosen by the autotuner: samples per lane,
+// minimum resident blocks per SM (register budget) and items per resident
+// warp (chunk granularity).
+struct TuneChoice {
+  uint32_t spl = 4;
+  uint32_t minb = 4;
+  uint32_t waves = 32;
+};
+
+// A captured plan/hash/finalize sequence, replayed for identical calls.
+struct GraphEntry {
+  std::vector<unsigned char> key;
+  cudaGraphExec_t exec = nullptr;
+};
+
 }  // namespace
 
 // The generator.  Opaque to callers (minhashcuda.h declares only the tag).
@@ -145,6 +161,12 @@ struct MinhashCudaGenerator_ {
   };
   mutable Slot slots[2];
   mutable cudaStream_t s_in = nullptr, s_out = nullptr;
+  // Autotuner results by shape class (see tune_key); read by every planner,
+  // including the server's lane threads, hence its own lock.
+  mutable std::mutex tune_mu;
+  mutable std::unordered_map<uint64_t, TuneChoice> tuned;
+  // CUDA graphs of mhcuda_calc_device calls, most recent last.
+  mutable std::vector<GraphEntry> graphs;
   // Optional timing of every hash-kernel launch with CUDA events recorded on
   // the launch stream (mhcuda_profile / mhcuda_profile_read).
   mutable bool profiling = false;
@@ -170,6 +192,7 @@ struct MinhashCudaGenerator_ {
     }
     if (s_in) cudaStreamDestroy(s_in);
     if (s_out) cudaStreamDestroy(s_out);
+    for (auto &g : graphs) cudaGraphExecDestroy(g.exec);
     if (params) cudaFree(params);
     if (stream) cudaStreamDestroy(stream);
   }
@@ -194,10 +217,39 @@ int pick_device(uint32_t devices) {
 }
 
 // Chooses samples-per-lane, chunk size and grid for one launch.
-HashPlan make_plan(const Gen *gen, uint64_t nnz, uint64_t rows) {
+// Key of the autotuner's table: the shape class of a launch (log2 of nnz and
+// of the mean row length).
+uint64_t tune_key(uint64_t nnz, uint64_t rows) {
+  auto lg = [](uint64_t x) {
+    uint64_t b = 0;
+    while (x > 1) {
+      x >>= 1;
+      ++b;
+    }
+    return b;
+  };
+  const uint64_t avg = rows ? (nnz + rows - 1) / rows : 1;
+  return (lg(nnz + 1) << 8) | lg(avg + 1);
+}
+
+HashPlan make_plan(const Gen *gen, uint64_t nnz, uint64_t rows, const TuneChoice *force = nullptr) {
   HashPlan p{};
   const uint32_t s_pad = gen->s_pad;
+  TuneChoice tuned{};
+  bool have_tuned = false;
+  if (force) {
+    tuned = *force;
+    have_tuned = true;
+  } else {
+    std::lock_guard<std::mutex> lock(gen->tune_mu);
+    const auto it = gen->tuned.find(tune_key(nnz, rows));
+    if (it != gen->tuned.end()) {
+      tuned = it->second;
+      have_tuned = true;
+    }
+  }
   int spl = env_int("MHCUDA_B200_SPL", 0);
+  if (have_tuned && spl == 0) spl = static_cast<int>(tuned.spl);
   if (spl != 1 && spl != 2 && spl != 4) {
     // Wide tiles amortise the per-nnz overhead (shuffles, addressing, the
     // logf share); narrow tiles give small inputs more warps.  Keep lane
@@ -215,7 +267,7 @@ HashPlan make_plan(const Gen *gen, uint64_t nnz, uint64_t rows) {
   p.spl = static_cast<uint32_t>(spl);
   p.minb = 4;
   if (p.spl == 4) {
-    const int minb = env_int("MHCUDA_B200_MINB", 4);
+    const int minb = env_int("MHCUDA_B200_MINB", have_tuned ? static_cast<int>(tuned.minb) : 4);
     p.minb = minb == 3 ? 3u : 4u;
   }
   const uint32_t tile_w = 32u * p.spl;
@@ -223,7 +275,8 @@ HashPlan make_plan(const Gen *gen, uint64_t nnz, uint64_t rows) {
   const int bps = mhb::hash_blocks_per_sm(p.spl, p.minb);
   const uint64_t resident_warps =
       static_cast<uint64_t>(gen->sm_count) * bps * (mhb::kHashBlock / 32);
-  const int waves = std::max(1, env_int("MHCUDA_B200_WAVES", 32));
+  const int waves = std::max(
+      1, env_int("MHCUDA_B200_WAVES", have_tuned ? static_cast<int>(tuned.waves) : 32));
   const uint64_t target_items = resident_warps * waves;
   uint64_t chunk = (nnz * p.ntiles + target_items - 1) / target_items;
   // Rows shorter than a chunk finish inside it; aim for a few rows per chunk.
@@ -727,7 +780,110 @@ enum MHCUDAResult mhcuda_calc_device(const MinhashCudaGenerator *gen, const floa
   a.cols = d_cols;
   a.indptr = d_rows;
   a.out = d_output;
-  return enqueue_hash(gen, a, plan, st);
+  // Repeated calls with identical arguments replay a CUDA graph of the
+  // memset + plan + hash + finalize sequence (one launch instead of four).
+  // Not while profiling (per-launch events) or while the caller's stream is
+  // itself being captured (the work then simply joins the caller's graph).
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  MHB_CHECK(gen, cudaStreamIsCapturing(st, &cap), mhcudaRuntimeError);
+  if (gen->profiling || cap != cudaStreamCaptureStatusNone ||
+      env_int("MHCUDA_B200_NO_GRAPHS", 0) != 0)
+    return enqueue_hash(gen, a, plan, st);
+  std::vector<unsigned char> key(sizeof(a) + sizeof(plan) + sizeof(st));
+  memcpy(key.data(), &a, sizeof(a));
+  memcpy(key.data() + sizeof(a), &plan, sizeof(plan));
+  memcpy(key.data() + sizeof(a) + sizeof(plan), &st, sizeof(st));
+  for (size_t i = 0; i < gen->graphs.size(); ++i) {
+    if (gen->graphs[i].key == key) {
+      MHB_CHECK(gen, cudaGraphLaunch(gen->graphs[i].exec, st), mhcudaRuntimeError);
+      return mhcudaSuccess;
+    }
+  }
+  cudaGraph_t graph = nullptr;
+  MHB_CHECK(gen, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), mhcudaRuntimeError);
+  r = enqueue_hash(gen, a, plan, st);
+  const cudaError_t end = cudaStreamEndCapture(st, &graph);
+  if (r != mhcudaSuccess || end != cudaSuccess) {
+    cudaGetLastError();
+    if (graph) cudaGraphDestroy(graph);
+    return r != mhcudaSuccess ? r : mhcudaRuntimeError;
+  }
+  GraphEntry e;
+  e.key = std::move(key);
+  const cudaError_t inst = cudaGraphInstantiate(&e.exec, graph, 0);
+  cudaGraphDestroy(graph);
+  MHB_CHECK(gen, inst, mhcudaRuntimeError);
+  constexpr size_t kMaxGraphs = 8;
+  if (gen->graphs.size() == kMaxGraphs) {
+    cudaGraphExecDestroy(gen->graphs.front().exec);
+    gen->graphs.erase(gen->graphs.begin());
+  }
+  gen->graphs.push_back(std::move(e));
+  MHB_CHECK(gen, cudaGraphLaunch(gen->graphs.back().exec, st), mhcudaRuntimeError);
+  return mhcudaSuccess;
+}
+
+enum MHCUDAResult mhcuda_autotune(const MinhashCudaGenerator *gen, const float *d_weights,
+                                  const uint32_t *d_cols, const uint32_t *d_rows, uint32_t length,
+                                  uint32_t nnz, uint32_t *d_output, void *stream,
+                                  uint32_t *choice, double *best_ms) {
+  if (!gen || !d_rows || !d_output || length == 0 || (nnz && (!d_weights || !d_cols)))
+    return mhcudaInvalidArguments;
+  std::lock_guard<std::mutex> lock(gen->mu);
+  MHB_CHECK(gen, cudaSetDevice(gen->device), mhcudaNoSuchDevice);
+  const cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : gen->stream;
+  // Candidates: samples per lane (lane utilisation of the last tile >= 1/2),
+  // register budget of the 4-sample variant, and chunk granularity.
+  std::vector<TuneChoice> cands;
+  for (uint32_t spl : {4u, 2u, 1u}) {
+    const uint32_t w = 32u * spl, tiles = (gen->s_pad + w - 1) / w;
+    if (static_cast<double>(gen->s_pad) / (static_cast<double>(tiles) * w) < 0.5) continue;
+    for (uint32_t minb : spl == 4 ? std::vector<uint32_t>{4u, 3u} : std::vector<uint32_t>{4u})
+      for (uint32_t waves : {8u, 32u, 128u}) cands.push_back(TuneChoice{spl, minb, waves});
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  MHB_CHECK(gen, cudaEventCreate(&e0), mhcudaRuntimeError);
+  MHB_CHECK(gen, cudaEventCreate(&e1), mhcudaRuntimeError);
+  TuneChoice best{};
+  double best_t = 1e300;
+  MHCUDAResult r = mhcudaSuccess;
+  for (const TuneChoice &c : cands) {
+    const HashPlan plan = make_plan(gen, nnz, length, &c);
+    HashArgs a{};
+    r = prepare_launch(gen, length, nnz, plan, &a);
+    if (r != mhcudaSuccess) break;
+    a.weights = d_weights;
+    a.cols = d_cols;
+    a.indptr = d_rows;
+    a.out = d_output;
+    r = enqueue_hash(gen, a, plan, st);  // warm-up
+    if (r != mhcudaSuccess) break;
+    MHB_CHECK(gen, cudaEventRecord(e0, st), mhcudaRuntimeError);
+    for (int k = 0; k < 2 && r == mhcudaSuccess; ++k) r = enqueue_hash(gen, a, plan, st);
+    MHB_CHECK(gen, cudaEventRecord(e1, st), mhcudaRuntimeError);
+    MHB_CHECK(gen, cudaEventSynchronize(e1), mhcudaRuntimeError);
+    float ms = 0.0f;
+    MHB_CHECK(gen, cudaEventElapsedTime(&ms, e0, e1), mhcudaRuntimeError);
+    MHB_DEBUG(gen, "autotune spl=%u minb=%u waves=%u: %.3f ms\n", c.spl, c.minb, c.waves, ms / 2);
+    if (ms / 2 < best_t) {
+      best_t = ms / 2;
+      best = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (r != mhcudaSuccess) return r;
+  {
+    std::lock_guard<std::mutex> tl(gen->tune_mu);
+    gen->tuned[tune_key(nnz, length)] = best;
+  }
+  if (choice) {
+    choice[0] = best.spl;
+    choice[1] = best.minb;
+    choice[2] = best.waves;
+  }
+  if (best_ms) *best_ms = best_t;
+  return read_status(gen, st);
 }
 
 enum MHCUDAResult mhcuda_device_status(const MinhashCudaGenerator *gen) {
