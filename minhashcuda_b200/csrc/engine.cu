@@ -418,11 +418,16 @@ MHCUDAResult calc_pipelined(const Gen *gen, const float *weights, const uint32_t
   const cudaStream_t st = gen->stream;
   MHB_CHECK(gen, batch_streams(gen), mhcudaRuntimeError);
   const uint64_t nnz = static_cast<uint64_t>(rows[length]) - rows[0];
-  uint64_t block_nnz = std::min<uint64_t>(std::max<uint64_t>(nnz / 8, 8ull << 20), 256ull << 20);
-  const int forced = env_int("MHCUDA_B200_BLOCK_NNZ", 0);
-  if (forced > 0) block_nnz = static_cast<uint64_t>(forced);
   const bool pin_in = is_pinned(weights) && is_pinned(cols) && is_pinned(rows);
   const bool pin_out = is_pinned(output);
+  // Page-locked inputs copy straight from the caller: large blocks.  Pageable
+  // ones go through pinned staging, which is cheaper to allocate (and
+  // re-fill) in smaller blocks.
+  uint64_t block_nnz =
+      pin_in ? std::min<uint64_t>(std::max<uint64_t>(nnz / 8, 8ull << 20), 256ull << 20)
+             : std::min<uint64_t>(std::max<uint64_t>(nnz / 16, 4ull << 20), 32ull << 20);
+  const int forced = env_int("MHCUDA_B200_BLOCK_NNZ", 0);
+  if (forced > 0) block_nnz = static_cast<uint64_t>(forced);
   const size_t row_bytes = static_cast<size_t>(gen->samples) * 2 * sizeof(uint32_t);
   MHB_CHECK(gen, gen->d_status.ensure(sizeof(uint32_t)), mhcudaMemoryAllocationFailure);
   MHB_CHECK(gen, cudaMemsetAsync(gen->d_status.ptr, 0, sizeof(uint32_t), st), mhcudaRuntimeError);

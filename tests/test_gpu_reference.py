@@ -162,7 +162,7 @@ def test_large_workload_slice_vs_reference_build():
     rows = int(os.environ.get("MHB_REF_ROWS", "200000"))
     ip, cols, wts = synth.host_csr(w, 0, rows)
     with _ref_gen(w.dim, w.samples, seed=w.seed) as ref:
-        ref.calc(wts, cols, ip[:2])  # warm-up on the first row
+        ref.calc(wts, cols, ip)  # warm-up with the same call
         t0 = time.perf_counter()
         rout = ref.calc(wts, cols, ip)
         t_ref = time.perf_counter() - t0
@@ -171,7 +171,7 @@ def test_large_workload_slice_vs_reference_build():
         got = eng.retrieve()
         for g, p in zip(got, params):
             np.testing.assert_array_equal(g.view(np.uint32), p.view(np.uint32))
-        eng.calc(wts, cols, ip[:2])
+        eng.calc(wts, cols, ip)  # warm-up with the same call
         t0 = time.perf_counter()
         eout = eng.calc(wts, cols, ip)
         t_eng = time.perf_counter() - t0
@@ -188,3 +188,97 @@ def test_large_workload_slice_vs_reference_build():
     if out:
         with open(out, "a") as f:
             f.write(json.dumps(rec) + "\n")
+
+
+def _record(rec):
+    import json
+    import os
+    print(json.dumps(rec))
+    out = os.environ.get("MHB_PERF_OUT")
+    if out:
+        with open(out, "a") as f:
+            f.write(json.dumps(rec) + "\n")
+
+
+def _timed(fn, reps):
+    import time
+    fn()
+    t = time.perf_counter()
+    for _ in range(reps):
+        r = fn()
+    return (time.perf_counter() - t) / reps, r
+
+
+@pytest.mark.gpu
+def test_small_config_timing_vs_reference_build():
+    """6400x130, 128 samples, seed 1 (test.py:92-101): one calc, host buffers."""
+    _, m = O.reference_small_matrix(1)
+    with _ref_gen(130, 128, seed=1) as ref, engine_gen(130, 128, seed=1) as eng:
+        t_ref, rout = _timed(lambda: ref.calc_csr(m), 20)
+        t_eng, eout = _timed(lambda: eng.calc_csr(m), 20)
+    mask = selected(eout)
+    np.testing.assert_array_equal(eout[mask], rout[mask])
+    _record({"test": "small_config", "rows": 6400, "nnz": int(m.nnz), "samples": 128,
+             "reference_s": t_ref, "engine_s": t_eng,
+             "reference_evals_per_s": m.nnz * 128 / t_ref, "engine_evals_per_s": m.nnz * 128 / t_eng})
+
+
+@pytest.mark.gpu
+def test_batched_subset_timing_vs_reference_build():
+    """The first 512 matrices of the uneven batch (2^20 dims, 256 samples):
+    the reference makes one calc per matrix; the engine both that way and
+    as one mhcuda_calc_batch."""
+    import ctypes
+    from minhashcuda_b200 import synth
+    w = synth.WORKLOADS["batched"]
+    shapes = synth.batched_shapes(w)[:512]
+    total = int(shapes.sum())
+    ip, cols, wts = synth.host_csr(w, 0, total)
+    base = np.concatenate([[0], np.cumsum(shapes)])
+    S = w.samples
+    with _ref_gen(w.dim, S, seed=w.seed) as ref, engine_gen(w.dim, S, seed=w.seed) as eng:
+        def plain(g):
+            outs = []
+            for i in range(len(shapes)):
+                outs.append(g.calc(wts, cols, ip[base[i]:base[i + 1] + 1]))
+            return outs
+        t_ref, rout = _timed(lambda: plain(ref), 1)
+        t_eng, eout = _timed(lambda: plain(eng), 1)
+        n = len(shapes)
+        P = ctypes.c_void_p
+        out_b = np.empty((total, S, 2), np.uint32)
+        rb = S * 8
+        W = (P * n)(*([wts.ctypes.data] * n))
+        C = (P * n)(*([cols.ctypes.data] * n))
+        R = (P * n)(*[ip.ctypes.data + 4 * int(b) for b in base[:-1]])
+        L = (ctypes.c_uint32 * n)(*[int(x) for x in shapes])
+        Ob = (P * n)(*[out_b.ctypes.data + rb * int(b) for b in base[:-1]])
+        t_bat, _ = _timed(lambda: eng.lib.mhcuda_calc_batch(eng.h, n, W, C, R, L, Ob), 3)
+    for r_, e_ in zip(rout, eout):
+        mask = selected(e_)
+        np.testing.assert_array_equal(e_[mask], r_[mask])
+    np.testing.assert_array_equal(np.concatenate(eout), out_b)
+    evals = int(ip[-1]) * S
+    _record({"test": "batched_subset", "matrices": n, "rows": total, "nnz": int(ip[-1]),
+             "samples": S, "reference_plain_s": t_ref, "engine_plain_s": t_eng,
+             "engine_batch_s": t_bat, "reference_plain_evals_per_s": evals / t_ref,
+             "engine_plain_evals_per_s": evals / t_eng, "engine_batch_evals_per_s": evals / t_bat})
+
+
+@pytest.mark.gpu
+def test_streamed_block_timing_vs_reference_build():
+    """One 524,288-row block of the row-streamed workload (12M dims, 128
+    samples, 18.4 GB of parameters): one calc each, host buffers."""
+    from minhashcuda_b200 import synth
+    w = synth.WORKLOADS["streamed"]
+    rows = w.extra["block_rows"]
+    ip, cols, wts = synth.host_csr(w, 0, rows)
+    with _ref_gen(w.dim, w.samples, seed=w.seed) as ref:
+        t_ref, rout = _timed(lambda: ref.calc(wts, cols, ip), 1)
+    with engine_gen(w.dim, w.samples, seed=w.seed) as eng:
+        t_eng, eout = _timed(lambda: eng.calc(wts, cols, ip), 3)
+    np.testing.assert_array_equal(eout, rout)
+    evals = int(ip[-1]) * w.samples
+    _record({"test": "streamed_block", "rows": rows, "nnz": int(ip[-1]), "samples": w.samples,
+             "dim": w.dim, "reference_s": t_ref, "engine_s": t_eng,
+             "reference_evals_per_s": evals / t_ref, "engine_evals_per_s": evals / t_eng})
