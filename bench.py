@@ -647,11 +647,8 @@ def main():
             pg.barrier()
 
     def max_over_ranks(x):
-        if not pg:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        return float(t.item())
+        from minhashcuda_b200.replicas import max_over_ranks as reduce_max
+        return reduce_max(x, pg, device="cuda")
 
     tuned = None
     if args.autotune:
