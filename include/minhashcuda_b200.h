@@ -111,6 +111,28 @@ enum MHCUDAResult mhcuda_profile(const MinhashCudaGenerator *gen, int enable);
 enum MHCUDAResult mhcuda_profile_read(const MinhashCudaGenerator *gen, double *hash_ms,
                                       uint64_t *launches);
 
+/* ---- Downstream of the hash (device-resident hashes) ---------------------
+ * d_hashes is [rows][samples][2] uint32 in the generator's device memory, as
+ * mhcuda_calc_device writes it.  Both calls wait for their kernel.  No
+ * counterpart in the reference, which returns the hashes to the host and
+ * leaves their use to the caller (its tests estimate Jaccard similarity from
+ * them, test.py:104-106). */
+
+/* LSH band keys: d_keys[row][b] (samples/band_width bands of band_width
+ * samples; trailing samples unused) is a 64-bit key of the band's (k, t)
+ * pairs: h = 0x6A09E667F3BCC909 ^ b, then h = splitmix64(h ^ (k << 32 | t))
+ * per sample.  Rows sharing a key in some band are candidate pairs. */
+enum MHCUDAResult mhcuda_lsh_bands(const MinhashCudaGenerator *gen, const uint32_t *d_hashes,
+                                   uint32_t rows, uint32_t band_width, uint64_t *d_keys,
+                                   void *stream);
+
+/* Weighted-Jaccard estimates: d_out[p] = fraction of samples whose (k, t)
+ * pairs are equal for rows d_pairs[2p] and d_pairs[2p+1] (-1 for a pair
+ * naming a row >= rows). */
+enum MHCUDAResult mhcuda_jaccard(const MinhashCudaGenerator *gen, const uint32_t *d_hashes,
+                                 uint32_t rows, const uint32_t *d_pairs, uint64_t npairs,
+                                 float *d_out, void *stream);
+
 /* ---- Serving: a continuous-batching request loop on one device ----------
  * No counterpart in the reference (every mhcuda_calc there is one blocking
  * launch per device, minhashcuda.cc:583-642).  A worker thread keeps `lanes`

@@ -38,7 +38,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-ccbin", HOST_CXX,
               "-I" + INCLUDE, "--expt-relaxed-constexpr"]
 
-ENGINE_SOURCES = ["hash_kernels.cu", "param_kernels.cu", "engine.cu", "noalloc.cu", "server.cu"]
+ENGINE_SOURCES = ["hash_kernels.cu", "param_kernels.cu", "engine.cu", "noalloc.cu", "server.cu",
+                  "lsh.cu"]
 HEADERS = ["wmh_internal.h"]
 
 EXT_SUFFIX = sysconfig.get_config_var("EXT_SUFFIX") or ".so"

@@ -119,6 +119,23 @@ bool is_csr(PyObject *m) {
   return false;
 }
 
+// A uint32 view of an index array.  Contiguous int32 arrays (scipy's default
+// index type) are used in place: the bits are the same for every valid index,
+// and a negative one reads as a column >= dim, which the device rejects.
+// Other types are cast (a copy), as python.cc:317,323 always does.
+Ref as_u32(PyObject *obj) {
+  if (PyArray_Check(obj)) {
+    PyArrayObject *a = reinterpret_cast<PyArrayObject *>(obj);
+    const int t = PyArray_TYPE(a);
+    if ((t == NPY_INT32 || t == NPY_UINT32) && PyArray_ISCARRAY_RO(a) &&
+        PyArray_ISNOTSWAPPED(a)) {
+      Py_INCREF(obj);
+      return Ref(obj);
+    }
+  }
+  return Ref(PyArray_FROM_OTF(obj, NPY_UINT32, NPY_ARRAY_FORCECAST | NPY_ARRAY_IN_ARRAY));
+}
+
 bool csr_view(PyObject *m, Csr *out) {
   if (!is_csr(m)) return false;
   Ref d(PyObject_GetAttrString(m, "data"));
@@ -129,15 +146,13 @@ bool csr_view(PyObject *m, Csr *out) {
     return false;
   }
   Ref i(PyObject_GetAttrString(m, "indices"));
-  if (i)
-    out->indices = Ref(PyArray_FROM_OTF(i.get(), NPY_UINT32, NPY_ARRAY_FORCECAST | NPY_ARRAY_IN_ARRAY));
+  if (i) out->indices = as_u32(i.get());
   if (!out->indices) {
     PyErr_SetString(PyExc_ValueError, "Failed to convert csr_matrix.indices to numpy.array");
     return false;
   }
   Ref p(PyObject_GetAttrString(m, "indptr"));
-  if (p)
-    out->indptr = Ref(PyArray_FROM_OTF(p.get(), NPY_UINT32, NPY_ARRAY_FORCECAST | NPY_ARRAY_IN_ARRAY));
+  if (p) out->indptr = as_u32(p.get());
   if (!out->indptr) {
     PyErr_SetString(PyExc_ValueError, "Failed to convert csr_matrix.indptr to numpy.array");
     return false;

@@ -259,3 +259,38 @@ FLOAT_V = [0, 1.0497366, 0.8494359, 0.66231006, 0.66231006, 0.8494359,
            0, 0.66231006, 0.33652836, 0, 0, 0.5359344,
            0.8494359, 0.66231006, 1.0497366, 0.33652836, 0.66231006, 0.8494359,
            0.6800841, 0.33652836]
+
+
+def _splitmix64(x):
+    """splitmix64 finaliser on uint64 numpy arrays (wrapping arithmetic)."""
+    x = (x + np.uint64(0x9E3779B97F4A7C15)).astype(np.uint64)
+    x = (x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+    x = (x ^ (x >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return x ^ (x >> np.uint64(31))
+
+
+def lsh_band_keys(hashes, band_width):
+    """Band keys of [rows][samples][2] uint32 hashes as the engine defines them:
+    h = 0x6A09E667F3BCC909 ^ b, then h = splitmix64(h ^ (k << 32 | t)) per
+    sample of band b.  Returns uint64 [rows][samples // band_width]."""
+    h = np.asarray(hashes, np.uint32)
+    rows, samples, _ = h.shape
+    bands = samples // band_width
+    kt = (h[..., 0].astype(np.uint64) << np.uint64(32)) | h[..., 1].astype(np.uint64)
+    out = np.empty((rows, bands), np.uint64)
+    with np.errstate(over="ignore"):
+        for b in range(bands):
+            key = np.full(rows, np.uint64(0x6A09E667F3BCC909) ^ np.uint64(b), np.uint64)
+            for s in range(b * band_width, (b + 1) * band_width):
+                key = _splitmix64(key ^ kt[:, s])
+            out[:, b] = key
+    return out
+
+
+def jaccard_estimate(hashes, pairs):
+    """Fraction of samples whose (k, t) pairs agree, per row pair (the
+    estimator of datasketch's WeightedMinHash.jaccard used by test.py:104-106)."""
+    h = np.asarray(hashes, np.uint32)
+    p = np.asarray(pairs, np.int64).reshape(-1, 2)
+    same = np.all(h[p[:, 0]] == h[p[:, 1]], axis=2)
+    return same.mean(axis=1).astype(np.float32)
