@@ -81,6 +81,34 @@ enum MHCUDAResult mhcuda_calc_device_noalloc(
     const uint32_t *d_cols, const uint32_t *d_rows, uint32_t length,
     uint32_t nnz, uint32_t *d_output, void *stream);
 
+/* Element types accepted by mhcuda_calc_typed. */
+enum MHCUDAElementType {
+  mhcudaFloat32 = 0,
+  mhcudaFloat64 = 1,
+  mhcudaUInt32 = 2,
+  mhcudaInt32 = 3,
+  mhcudaInt64 = 4,
+  mhcudaUInt64 = 5
+};
+
+/* mhcuda_calc (minhashcuda.h:115-118) for CSR arrays in the element types
+ * scipy produces: float64 data, and int64 indices and offsets once a matrix
+ * has 2^31 nnz or more.  weights: mhcudaFloat32/Float64; cols and rows: any
+ * of the integer types.  The reference casts whole arrays to float32/uint32
+ * on the host before its call (python.cc:310-327); here each block of rows is
+ * converted while it is staged into page-locked memory on host threads, so
+ * nothing is copied whole.  float64 -> float32 rounds to nearest (numpy's
+ * astype).  Offsets are taken relative to rows[0], so a row range of a matrix
+ * with more than 2^32 nnz works as long as the range itself has fewer.
+ * Returns mhcudaInvalidArguments for an unknown type, an offset that
+ * decreases or spans 2^32 or more, and a column outside [0, dim) (the
+ * reference's cast wraps such values, python.cc:317-323).  Results equal
+ * mhcuda_calc on the converted arrays. */
+enum MHCUDAResult mhcuda_calc_typed(
+    const MinhashCudaGenerator *gen, const void *weights, int weights_type,
+    const void *cols, int cols_type, const void *rows, int rows_type,
+    uint32_t length, uint32_t *output);
+
 /* Hashes `count` independent CSR matrices (host buffers, as in mhcuda_calc)
  * against one generator in one device pass: the matrices are staged
  * back to back, one persistent launch walks a (matrix, row-chunk) work list

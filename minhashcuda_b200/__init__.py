@@ -30,6 +30,9 @@ from . import libMHCUDA  # noqa: E402  (the CPython extension next to this file)
 
 sys.modules.setdefault("libMHCUDA", libMHCUDA)
 
+# MHCUDAElementType (include/minhashcuda_b200.h)
+FLOAT32, FLOAT64, UINT32, INT32, INT64, UINT64 = range(6)
+
 # MHCUDAResult (include/minhashcuda.h)
 SUCCESS = 0
 INVALID_ARGUMENTS = 1
@@ -66,6 +69,8 @@ SIGNATURES = {
     "mhcuda_autotune": (_RES, [_P, _P, _P, _P, _U32, _U32, _P, _P,
                                ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_double)]),
     "mhcuda_calc_device_noalloc": (_RES, [_P, _P, _P, _P, _U32, _U32, _P, _P]),
+    "mhcuda_calc_typed": (_RES, [_P, _P, ctypes.c_int, _P, ctypes.c_int, _P, ctypes.c_int, _U32,
+                                 _P]),
     "mhcuda_calc_batch": (_RES, [_P, _U32, _P, _P, _P, _P, _P]),
     "mhcuda_debug_device_logf": (_RES, [_U32, _P, _P, ctypes.c_uint64]),
     "mhcuda_lsh_bands": (_RES, [_P, _P, _U32, _U32, _P, _P]),

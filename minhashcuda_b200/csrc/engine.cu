@@ -369,12 +369,20 @@ bool is_pinned(const void *p) {
   return attr.type == cudaMemoryTypeHost;
 }
 
+// Host threads for staging copies and conversions: one per core up to 16
+// (a 16-core host stages pageable float64/int64 input 1.36x faster with 16
+// than with 8); MHCUDA_B200_HOST_THREADS overrides.
+unsigned host_threads() {
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const int forced = env_int("MHCUDA_B200_HOST_THREADS", 0);
+  return forced > 0 ? static_cast<unsigned>(forced) : std::min(16u, hw);
+}
+
 // memcpy split over a few threads for large blocks (host bandwidth for the
 // pinned staging of pageable caller buffers).
 void par_memcpy(void *dst, const void *src, size_t bytes) {
   const size_t kSplit = static_cast<size_t>(8) << 20;
-  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-  const unsigned n = bytes < kSplit ? 1u : std::min<unsigned>(8u, hw);
+  const unsigned n = bytes < kSplit ? 1u : host_threads();
   if (n == 1) {
     memcpy(dst, src, bytes);
     return;
@@ -413,12 +421,84 @@ constexpr uint64_t kPipelineMinNnz = 16ull << 20;
 // block i+1 is copied in on s_in and block i-1's hashes are copied out on
 // s_out.  Caller buffers that are page-locked are copied directly; pageable
 // ones go through pinned staging filled by host threads.
-MHCUDAResult calc_pipelined(const Gen *gen, const float *weights, const uint32_t *cols,
-                            const uint32_t *rows, uint32_t length, uint32_t *output) {
+// A caller's host CSR: float32 or float64 weights, 32-bit (uint32/int32 bits)
+// or 64-bit columns, uint32 offsets (absolute: weights[rows[0]] is the first
+// entry).
+struct HostCsr {
+  const void *weights;
+  bool w64;
+  const void *cols;
+  int cols64;  // 0: 32-bit, 1: int64, 2: uint64
+  const uint32_t *rows;
+  bool native() const { return !w64 && cols64 == 0; }
+};
+
+// Runs f(begin, end) over [0, n), split over up to 8 host threads once n
+// reaches `split`.
+template <typename F>
+void par_for(size_t n, size_t split, F f) {
+  const unsigned k = n < split ? 1u : host_threads();
+  if (k == 1) {
+    if (n) f(size_t{0}, n);
+    return;
+  }
+  const size_t part = (((n + k - 1) / k) + 1023) & ~static_cast<size_t>(1023);
+  std::vector<std::thread> pool;
+  for (unsigned t = 0; t < k; ++t) {
+    const size_t b = t * part;
+    if (b >= n) break;
+    const size_t e = std::min(n, b + part);
+    pool.emplace_back([=]() { f(b, e); });
+  }
+  for (auto &th : pool) th.join();
+}
+
+// Stages entries [b0, b0 + n) of the caller's weights and columns into the
+// page-locked float32/uint32 buffers, converting on the way: float64 rounds
+// to nearest; a 64-bit column outside [0, 2^32) becomes 0xFFFFFFFF, which no
+// dim admits, so the device check rejects it instead of a wrapped value
+// passing.
+void stage_entries(const HostCsr &in, uint64_t b0, size_t n, float *w, uint32_t *c) {
+  constexpr size_t kSplit = size_t{2} << 20;
+  if (in.w64) {
+    const double *src = static_cast<const double *>(in.weights) + b0;
+    par_for(n, kSplit, [=](size_t b, size_t e) {
+      for (size_t i = b; i < e; ++i) w[i] = static_cast<float>(src[i]);
+    });
+  } else {
+    par_memcpy(w, static_cast<const float *>(in.weights) + b0, n * sizeof(float));
+  }
+  if (in.cols64 == 1) {
+    const int64_t *src = static_cast<const int64_t *>(in.cols) + b0;
+    par_for(n, kSplit, [=](size_t b, size_t e) {
+      for (size_t i = b; i < e; ++i) {
+        const int64_t v = src[i];
+        c[i] = (v < 0 || v > 0xFFFFFFFFll) ? 0xFFFFFFFFu : static_cast<uint32_t>(v);
+      }
+    });
+  } else if (in.cols64 == 2) {
+    const uint64_t *src = static_cast<const uint64_t *>(in.cols) + b0;
+    par_for(n, kSplit, [=](size_t b, size_t e) {
+      for (size_t i = b; i < e; ++i) {
+        const uint64_t v = src[i];
+        c[i] = v > 0xFFFFFFFFull ? 0xFFFFFFFFu : static_cast<uint32_t>(v);
+      }
+    });
+  } else {
+    par_memcpy(c, static_cast<const uint32_t *>(in.cols) + b0, n * sizeof(uint32_t));
+  }
+}
+
+MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
+                            uint32_t *output) {
   const cudaStream_t st = gen->stream;
   MHB_CHECK(gen, batch_streams(gen), mhcudaRuntimeError);
+  const uint32_t *rows = in.rows;
   const uint64_t nnz = static_cast<uint64_t>(rows[length]) - rows[0];
-  const bool pin_in = is_pinned(weights) && is_pinned(cols) && is_pinned(rows);
+  // Page-locked native arrays are copied straight from the caller; anything
+  // else is staged (and converted) block by block.
+  const bool pin_in = in.native() && is_pinned(in.weights) && is_pinned(in.cols) &&
+                      is_pinned(rows);
   const bool pin_out = is_pinned(output);
   // Page-locked inputs copy straight from the caller: large blocks.  Pageable
   // ones go through pinned staging, which is cheaper to allocate (and
@@ -461,14 +541,16 @@ MHCUDAResult calc_pipelined(const Gen *gen, const float *weights, const uint32_t
     MHB_CHECK(gen, sl.c.ensure(static_cast<size_t>(n) * 4 + 16), mhcudaMemoryAllocationFailure);
     MHB_CHECK(gen, sl.ip.ensure((static_cast<size_t>(len) + 1) * 4), mhcudaMemoryAllocationFailure);
     MHB_CHECK(gen, sl.out.ensure(len * row_bytes), mhcudaMemoryAllocationFailure);
-    const void *src_w = weights + b0, *src_c = cols + b0, *src_i = rows + r0;
-    if (!pin_in) {
+    const void *src_w = nullptr, *src_c = nullptr, *src_i = rows + r0;
+    if (pin_in) {
+      src_w = static_cast<const float *>(in.weights) + b0;
+      src_c = static_cast<const uint32_t *>(in.cols) + b0;
+    } else {
       MHB_CHECK(gen, sl.hw.ensure(static_cast<size_t>(n) * 4), mhcudaMemoryAllocationFailure);
       MHB_CHECK(gen, sl.hc.ensure(static_cast<size_t>(n) * 4), mhcudaMemoryAllocationFailure);
       MHB_CHECK(gen, sl.hip.ensure((static_cast<size_t>(len) + 1) * 4),
                 mhcudaMemoryAllocationFailure);
-      par_memcpy(sl.hw.ptr, src_w, static_cast<size_t>(n) * 4);
-      par_memcpy(sl.hc.ptr, src_c, static_cast<size_t>(n) * 4);
+      stage_entries(in, b0, n, static_cast<float *>(sl.hw.ptr), static_cast<uint32_t *>(sl.hc.ptr));
       memcpy(sl.hip.ptr, src_i, (static_cast<size_t>(len) + 1) * 4);
       src_w = sl.hw.ptr;
       src_c = sl.hc.ptr;
@@ -528,47 +610,82 @@ MHCUDAResult calc_pipelined(const Gen *gen, const float *weights, const uint32_t
   return read_status(gen, st);
 }
 
+// Scratch per buffer when the [samples][dim] parameter streams are handled a
+// block of sample rows at a time (init, retrieve, assign).
+constexpr uint64_t kParamChunkBytes = 1ull << 30;
+
+// Sample rows per block: about kParamChunkBytes of floats, whole 8-row groups
+// (32-byte write segments in the table) when a block holds 8 rows or more.
+// MHCUDA_B200_PARAM_CHUNK_ROWS overrides.
+uint32_t param_chunk_rows(uint32_t dim, uint32_t samples) {
+  const int forced = env_int("MHCUDA_B200_PARAM_CHUNK_ROWS", 0);
+  uint64_t rows = forced > 0 ? static_cast<uint64_t>(forced)
+                             : kParamChunkBytes / (static_cast<uint64_t>(dim) * sizeof(float));
+  if (forced <= 0 && rows >= 8) rows &= ~uint64_t{7};
+  return static_cast<uint32_t>(std::min<uint64_t>(std::max<uint64_t>(rows, 1), samples));
+}
+
+// Fills the table from `seed` as minhashcuda.cc:179-199 does: one cuRAND
+// generator of type CURAND_RNG_PSEUDO_DEFAULT draws five runs of dim*samples
+// uniforms U1..U5, and rs = -logf(U2*U1), ln_cs = logf(-logf(U3*U4)),
+// betas = U5, each run in [samples][dim] order.  The runs are not
+// materialised whole: two generators with that seed start at the absolute
+// offsets of a run pair (curandSetGeneratorOffset: draws k and k+1 begin at
+// k*n and (k+1)*n), each produces its run a block of sample rows at a time,
+// and every block is combined and transposed into the table at once.  Values
+// at an absolute offset do not depend on how the sequence is split into
+// calls, so the table equals the reference's bit for bit with scratch of two
+// blocks instead of two full runs (2 x 17 GB at 2^24 x 256).
 MHCUDAResult init_params(Gen *gen, uint32_t seed) {
-  const size_t n = static_cast<size_t>(gen->dim) * gen->samples;
+  const uint32_t D = gen->dim, S = gen->samples, P = gen->s_pad;
+  const uint64_t n = static_cast<uint64_t>(D) * S;
+  const uint32_t rows = param_chunk_rows(D, S);
+  const size_t block = static_cast<size_t>(rows) * D;
   DevBuf a, b;
-  MHB_CHECK(gen, a.ensure(n * sizeof(float)), mhcudaMemoryAllocationFailure);
-  MHB_CHECK(gen, b.ensure(n * sizeof(float)), mhcudaMemoryAllocationFailure);
-  curandGenerator_t rng = nullptr;
-  auto fail = [&](MHCUDAResult code) {
-    if (rng) curandDestroyGenerator(rng);
+  MHB_CHECK(gen, a.ensure(block * sizeof(float)), mhcudaMemoryAllocationFailure);
+  MHB_CHECK(gen, b.ensure(block * sizeof(float)), mhcudaMemoryAllocationFailure);
+  curandGenerator_t rng[2] = {nullptr, nullptr};
+  auto finish = [&](MHCUDAResult code) {
+    for (curandGenerator_t g : rng)
+      if (g) curandDestroyGenerator(g);
     return code;
   };
-  // The same generator type, seed and five draws of n floats as
-  // minhashcuda.cc:181-199, so a seed reproduces the reference's table.
-  if (curandCreateGenerator(&rng, CURAND_RNG_PSEUDO_DEFAULT) != CURAND_STATUS_SUCCESS)
-    return fail(mhcudaRuntimeError);
-  if (curandSetStream(rng, gen->stream) != CURAND_STATUS_SUCCESS ||
-      curandSetPseudoRandomGeneratorSeed(rng, seed) != CURAND_STATUS_SUCCESS)
-    return fail(mhcudaRuntimeError);
+  for (curandGenerator_t &g : rng) {
+    if (curandCreateGenerator(&g, CURAND_RNG_PSEUDO_DEFAULT) != CURAND_STATUS_SUCCESS) {
+      g = nullptr;
+      return finish(mhcudaRuntimeError);
+    }
+    if (curandSetStream(g, gen->stream) != CURAND_STATUS_SUCCESS ||
+        curandSetPseudoRandomGeneratorSeed(g, seed) != CURAND_STATUS_SUCCESS)
+      return finish(mhcudaRuntimeError);
+  }
+  struct Pass {
+    mhb::PairOp op;
+    uint32_t which;     // table slot: 0 rs, 1 ln_cs, 2 betas
+    uint64_t first;     // index of the first uniform run it consumes
+    bool pair;          // consumes runs first and first+1
+  };
+  const Pass passes[3] = {{mhb::PairOp::kGamma, 0, 0, true},
+                          {mhb::PairOp::kLogGamma, 1, 2, true},
+                          {mhb::PairOp::kCopy, 2, 4, false}};
   float *A = a.as<float>(), *B = b.as<float>();
-  const uint32_t D = gen->dim, S = gen->samples, P = gen->s_pad;
-  // rs = -logf(U2 * U1)
-  if (curandGenerateUniform(rng, A, n) != CURAND_STATUS_SUCCESS ||
-      curandGenerateUniform(rng, B, n) != CURAND_STATUS_SUCCESS)
-    return fail(mhcudaRuntimeError);
-  if (mhb::launch_pack_params(A, B, mhb::PairOp::kGamma, 0, D, S, P, gen->params, gen->stream) !=
-      cudaSuccess)
-    return fail(mhcudaRuntimeError);
-  // ln_cs = logf(-logf(U3 * U4))
-  if (curandGenerateUniform(rng, A, n) != CURAND_STATUS_SUCCESS ||
-      curandGenerateUniform(rng, B, n) != CURAND_STATUS_SUCCESS)
-    return fail(mhcudaRuntimeError);
-  if (mhb::launch_pack_params(A, B, mhb::PairOp::kLogGamma, 1, D, S, P, gen->params,
-                              gen->stream) != cudaSuccess)
-    return fail(mhcudaRuntimeError);
-  // betas = U5
-  if (curandGenerateUniform(rng, A, n) != CURAND_STATUS_SUCCESS) return fail(mhcudaRuntimeError);
-  if (mhb::launch_pack_params(A, nullptr, mhb::PairOp::kCopy, 2, D, S, P, gen->params,
-                              gen->stream) != cudaSuccess)
-    return fail(mhcudaRuntimeError);
-  if (cudaStreamSynchronize(gen->stream) != cudaSuccess) return fail(mhcudaRuntimeError);
-  curandDestroyGenerator(rng);
-  return mhcudaSuccess;
+  for (const Pass &p : passes) {
+    if (curandSetGeneratorOffset(rng[0], p.first * n) != CURAND_STATUS_SUCCESS ||
+        (p.pair && curandSetGeneratorOffset(rng[1], (p.first + 1) * n) != CURAND_STATUS_SUCCESS))
+      return finish(mhcudaRuntimeError);
+    for (uint32_t s0 = 0; s0 < S; s0 += rows) {
+      const uint32_t cnt = std::min(rows, S - s0);
+      const size_t len = static_cast<size_t>(cnt) * D;
+      if (curandGenerateUniform(rng[0], A, len) != CURAND_STATUS_SUCCESS ||
+          (p.pair && curandGenerateUniform(rng[1], B, len) != CURAND_STATUS_SUCCESS))
+        return finish(mhcudaRuntimeError);
+      if (mhb::launch_pack_params(A, p.pair ? B : nullptr, p.op, p.which, D, s0, cnt, P,
+                                  gen->params, gen->stream) != cudaSuccess)
+        return finish(mhcudaRuntimeError);
+    }
+  }
+  if (cudaStreamSynchronize(gen->stream) != cudaSuccess) return finish(mhcudaRuntimeError);
+  return finish(mhcudaSuccess);
 }
 
 }  // namespace
@@ -675,19 +792,26 @@ enum MHCUDAResult mhcuda_retrieve_random_vars(const MinhashCudaGenerator *gen, f
   if (!gen || !rs || !ln_cs || !betas) return mhcudaInvalidArguments;
   std::lock_guard<std::mutex> lock(gen->mu);
   MHB_CHECK(gen, cudaSetDevice(gen->device), mhcudaNoSuchDevice);
-  const size_t n = static_cast<size_t>(gen->dim) * gen->samples;
+  const uint32_t D = gen->dim, S = gen->samples;
+  const uint32_t rows = param_chunk_rows(D, S);
   DevBuf tmp;
-  MHB_CHECK(gen, tmp.ensure(n * sizeof(float)), mhcudaMemoryAllocationFailure);
+  MHB_CHECK(gen, tmp.ensure(static_cast<size_t>(rows) * D * sizeof(float)),
+            mhcudaMemoryAllocationFailure);
   float *dst[3] = {rs, ln_cs, betas};
+  // [samples][dim] host arrays, filled a block of sample rows at a time.
   for (uint32_t which = 0; which < 3; ++which) {
-    MHB_CHECK(gen, mhb::launch_unpack_params(gen->params, which, gen->dim, gen->samples,
-                                             gen->s_pad, tmp.as<float>(), gen->stream),
-              mhcudaRuntimeError);
-    MHB_CHECK(gen, cudaMemcpyAsync(dst[which], tmp.ptr, n * sizeof(float),
-                                   cudaMemcpyDeviceToHost, gen->stream),
-              mhcudaMemoryCopyError);
-    MHB_CHECK(gen, cudaStreamSynchronize(gen->stream), mhcudaMemoryCopyError);
+    for (uint32_t s0 = 0; s0 < S; s0 += rows) {
+      const uint32_t cnt = std::min(rows, S - s0);
+      const size_t len = static_cast<size_t>(cnt) * D;
+      MHB_CHECK(gen, mhb::launch_unpack_params(gen->params, which, D, s0, cnt, gen->s_pad,
+                                               tmp.as<float>(), gen->stream),
+                mhcudaRuntimeError);
+      MHB_CHECK(gen, cudaMemcpyAsync(dst[which] + static_cast<size_t>(s0) * D, tmp.ptr,
+                                     len * sizeof(float), cudaMemcpyDeviceToHost, gen->stream),
+                mhcudaMemoryCopyError);
+    }
   }
+  MHB_CHECK(gen, cudaStreamSynchronize(gen->stream), mhcudaMemoryCopyError);
   return mhcudaSuccess;
 }
 
@@ -696,20 +820,25 @@ enum MHCUDAResult mhcuda_assign_random_vars(const MinhashCudaGenerator *gen, con
   if (!gen || !rs || !ln_cs || !betas) return mhcudaInvalidArguments;
   std::lock_guard<std::mutex> lock(gen->mu);
   MHB_CHECK(gen, cudaSetDevice(gen->device), mhcudaNoSuchDevice);
-  const size_t n = static_cast<size_t>(gen->dim) * gen->samples;
+  const uint32_t D = gen->dim, S = gen->samples;
+  const uint32_t rows = param_chunk_rows(D, S);
   DevBuf tmp;
-  MHB_CHECK(gen, tmp.ensure(n * sizeof(float)), mhcudaMemoryAllocationFailure);
+  MHB_CHECK(gen, tmp.ensure(static_cast<size_t>(rows) * D * sizeof(float)),
+            mhcudaMemoryAllocationFailure);
   const float *src[3] = {rs, ln_cs, betas};
   for (uint32_t which = 0; which < 3; ++which) {
-    MHB_CHECK(gen, cudaMemcpyAsync(tmp.ptr, src[which], n * sizeof(float),
-                                   cudaMemcpyHostToDevice, gen->stream),
-              mhcudaMemoryCopyError);
-    MHB_CHECK(gen, mhb::launch_pack_params(tmp.as<float>(), nullptr, mhb::PairOp::kCopy, which,
-                                           gen->dim, gen->samples, gen->s_pad, gen->params,
-                                           gen->stream),
-              mhcudaRuntimeError);
-    MHB_CHECK(gen, cudaStreamSynchronize(gen->stream), mhcudaMemoryCopyError);
+    for (uint32_t s0 = 0; s0 < S; s0 += rows) {
+      const uint32_t cnt = std::min(rows, S - s0);
+      const size_t len = static_cast<size_t>(cnt) * D;
+      MHB_CHECK(gen, cudaMemcpyAsync(tmp.ptr, src[which] + static_cast<size_t>(s0) * D,
+                                     len * sizeof(float), cudaMemcpyHostToDevice, gen->stream),
+                mhcudaMemoryCopyError);
+      MHB_CHECK(gen, mhb::launch_pack_params(tmp.as<float>(), nullptr, mhb::PairOp::kCopy, which,
+                                             D, s0, cnt, gen->s_pad, gen->params, gen->stream),
+                mhcudaRuntimeError);
+    }
   }
+  MHB_CHECK(gen, cudaStreamSynchronize(gen->stream), mhcudaMemoryCopyError);
   return mhcudaSuccess;
 }
 
@@ -726,7 +855,7 @@ enum MHCUDAResult mhcuda_calc(const MinhashCudaGenerator *gen, const float *weig
   const int min_override = env_int("MHCUDA_B200_PIPELINE_MIN_NNZ", 0);
   const uint64_t pipe_min = min_override > 0 ? static_cast<uint64_t>(min_override) : kPipelineMinNnz;
   if (nnz >= pipe_min && env_int("MHCUDA_B200_NO_PIPELINE", 0) == 0)
-    return calc_pipelined(gen, weights, cols, rows, length, output);
+    return calc_pipelined(gen, HostCsr{weights, false, cols, 0, rows}, length, output);
   MHB_CHECK(gen, gen->d_weights.ensure(static_cast<size_t>(nnz) * 4 + 16),
             mhcudaMemoryAllocationFailure);
   MHB_CHECK(gen, gen->d_cols.ensure(static_cast<size_t>(nnz) * 4 + 16),
@@ -766,6 +895,55 @@ enum MHCUDAResult mhcuda_calc(const MinhashCudaGenerator *gen, const float *weig
   if (r != mhcudaSuccess) return r;
   MHB_INFO(gen, "mhcuda - success\n");
   return mhcudaSuccess;
+}
+
+enum MHCUDAResult mhcuda_calc_typed(const MinhashCudaGenerator *gen, const void *weights,
+                                    int weights_type, const void *cols, int cols_type,
+                                    const void *rows, int rows_type, uint32_t length,
+                                    uint32_t *output) {
+  if (!gen || !weights || !cols || !rows || !output || length == 0) return mhcudaInvalidArguments;
+  if (weights_type != mhcudaFloat32 && weights_type != mhcudaFloat64) return mhcudaInvalidArguments;
+  auto is_int = [](int t) {
+    return t == mhcudaUInt32 || t == mhcudaInt32 || t == mhcudaInt64 || t == mhcudaUInt64;
+  };
+  if (!is_int(cols_type) || !is_int(rows_type)) return mhcudaInvalidArguments;
+  const bool w64 = weights_type == mhcudaFloat64;
+  const int cols64 = cols_type == mhcudaInt64 ? 1 : cols_type == mhcudaUInt64 ? 2 : 0;
+  // 64-bit offsets are rebased to rows[0] (the caller's arrays are entered at
+  // that entry); 32-bit ones stay absolute, as mhcuda_calc takes them.
+  uint64_t base = 0;
+  std::vector<uint32_t> rebased;
+  const uint32_t *r32 = static_cast<const uint32_t *>(rows);
+  if (rows_type == mhcudaInt64 || rows_type == mhcudaUInt64) {
+    const bool sgn = rows_type == mhcudaInt64;
+    auto at = [&](uint32_t i) -> uint64_t {
+      return sgn ? static_cast<uint64_t>(static_cast<const int64_t *>(rows)[i])
+                 : static_cast<const uint64_t *>(rows)[i];
+    };
+    if (sgn && static_cast<const int64_t *>(rows)[0] < 0) return mhcudaInvalidArguments;
+    base = at(0);
+    rebased.resize(static_cast<size_t>(length) + 1);
+    uint64_t prev = base;
+    for (uint32_t i = 0; i <= length; ++i) {
+      const uint64_t v = at(i);
+      if ((sgn && static_cast<int64_t>(v) < 0) || v < prev || v - base > 0xFFFFFFFFull)
+        return mhcudaInvalidArguments;
+      rebased[i] = static_cast<uint32_t>(v - base);
+      prev = v;
+    }
+    r32 = rebased.data();
+  }
+  const size_t wsize = w64 ? sizeof(double) : sizeof(float);
+  const size_t csize = cols64 ? sizeof(uint64_t) : sizeof(uint32_t);
+  const void *w = static_cast<const char *>(weights) + base * wsize;
+  const void *c = static_cast<const char *>(cols) + base * csize;
+  if (!w64 && !cols64)
+    return mhcuda_calc(gen, static_cast<const float *>(w), static_cast<const uint32_t *>(c), r32,
+                       length, output);
+  std::lock_guard<std::mutex> lock(gen->mu);
+  MHB_CHECK(gen, cudaSetDevice(gen->device), mhcudaNoSuchDevice);
+  if (r32[length] < r32[0]) return mhcudaInvalidArguments;
+  return calc_pipelined(gen, HostCsr{w, w64, c, cols64, r32}, length, output);
 }
 
 enum MHCUDAResult mhcuda_calc_device(const MinhashCudaGenerator *gen, const float *d_weights,
@@ -927,7 +1105,7 @@ enum MHCUDAResult mhcuda_calc_batch(const MinhashCudaGenerator *gen, uint32_t co
   const uint64_t group_rows = 1u << 20;
   MHB_CHECK(gen, gen->d_status.ensure(sizeof(uint32_t)), mhcudaMemoryAllocationFailure);
   MHB_CHECK(gen, cudaMemsetAsync(gen->d_status.ptr, 0, sizeof(uint32_t), st), mhcudaRuntimeError);
-  const unsigned nth = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+  const unsigned nth = host_threads();
 
   // A slot's staged hashes go back to their matrices once its copy is done.
   struct Pending {

@@ -35,10 +35,11 @@ __device__ __forceinline__ float pair_op(PairOp op, float a, float b) {
   }
 }
 
-// Block (32, 8): tile of 32 samples x 32 columns.
+// Block (32, 8): tile of 32 samples x 32 columns.  a and b hold `samples`
+// rows of `dim` values, the rows s_base.. of the [samples][dim] streams.
 __global__ void pack_kernel(const float *__restrict__ a, const float *__restrict__ b, PairOp op,
-                            uint32_t which, uint32_t dim, uint32_t samples, uint32_t s_pad,
-                            float *__restrict__ params) {
+                            uint32_t which, uint32_t dim, uint32_t s_base, uint32_t samples,
+                            uint32_t s_pad, float *__restrict__ params) {
   __shared__ float tile[kTile][kTile + 1];
   const uint32_t d0 = blockIdx.x * kTile;
   const uint32_t s0 = blockIdx.y * kTile;
@@ -55,19 +56,20 @@ __global__ void pack_kernel(const float *__restrict__ a, const float *__restrict
   for (int k = threadIdx.y; k < kTile; k += kRowsPerPass) {
     const uint32_t d = d0 + k, s = s0 + threadIdx.x;
     if (d < dim && s < samples)
-      params[(static_cast<size_t>(d) * 3 + which) * s_pad + s] = tile[threadIdx.x][k];
+      params[(static_cast<size_t>(d) * 3 + which) * s_pad + s_base + s] = tile[threadIdx.x][k];
   }
 }
 
 __global__ void unpack_kernel(const float *__restrict__ params, uint32_t which, uint32_t dim,
-                              uint32_t samples, uint32_t s_pad, float *__restrict__ dst) {
+                              uint32_t s_base, uint32_t samples, uint32_t s_pad,
+                              float *__restrict__ dst) {
   __shared__ float tile[kTile][kTile + 1];
   const uint32_t d0 = blockIdx.x * kTile;
   const uint32_t s0 = blockIdx.y * kTile;
   for (int k = threadIdx.y; k < kTile; k += kRowsPerPass) {
     const uint32_t d = d0 + k, s = s0 + threadIdx.x;
     if (d < dim && s < samples)
-      tile[k][threadIdx.x] = params[(static_cast<size_t>(d) * 3 + which) * s_pad + s];
+      tile[k][threadIdx.x] = params[(static_cast<size_t>(d) * 3 + which) * s_pad + s_base + s];
   }
   __syncthreads();
   for (int k = threadIdx.y; k < kTile; k += kRowsPerPass) {
@@ -79,22 +81,22 @@ __global__ void unpack_kernel(const float *__restrict__ params, uint32_t which, 
 }  // namespace
 
 cudaError_t launch_pack_params(const float *a, const float *b, PairOp op, uint32_t which,
-                               uint32_t dim, uint32_t samples, uint32_t s_pad, float *params,
-                               cudaStream_t stream) {
+                               uint32_t dim, uint32_t s_base, uint32_t samples, uint32_t s_pad,
+                               float *params, cudaStream_t stream) {
   const dim3 block(kTile, kRowsPerPass);
   const dim3 grid((dim + kTile - 1) / kTile, (samples + kTile - 1) / kTile);
   if (grid.x == 0 || grid.y == 0) return cudaSuccess;
-  pack_kernel<<<grid, block, 0, stream>>>(a, b, op, which, dim, samples, s_pad, params);
+  pack_kernel<<<grid, block, 0, stream>>>(a, b, op, which, dim, s_base, samples, s_pad, params);
   return cudaGetLastError();
 }
 
 cudaError_t launch_unpack_params(const float *params, uint32_t which, uint32_t dim,
-                                 uint32_t samples, uint32_t s_pad, float *dst,
+                                 uint32_t s_base, uint32_t samples, uint32_t s_pad, float *dst,
                                  cudaStream_t stream) {
   const dim3 block(kTile, kRowsPerPass);
   const dim3 grid((dim + kTile - 1) / kTile, (samples + kTile - 1) / kTile);
   if (grid.x == 0 || grid.y == 0) return cudaSuccess;
-  unpack_kernel<<<grid, block, 0, stream>>>(params, which, dim, samples, s_pad, dst);
+  unpack_kernel<<<grid, block, 0, stream>>>(params, which, dim, s_base, samples, s_pad, dst);
   return cudaGetLastError();
 }
 

@@ -90,12 +90,15 @@ MinhashCudaGenerator *gen_from(unsigned long long v) {
   return gen;
 }
 
-// A CSR matrix viewed as the three C arrays mhcuda_calc takes.
+// A CSR matrix viewed as three C arrays and their element types
+// (MHCUDAElementType).  For mhcuda_calc_batch they are always
+// float32/uint32-bit; for mhcuda_calc_typed also float64 and 64-bit.
 struct Csr {
   Ref data, indices, indptr;
-  const float *weights = nullptr;
-  const uint32_t *cols = nullptr;
-  const uint32_t *rows = nullptr;
+  const void *weights = nullptr;
+  const void *cols = nullptr;
+  const void *rows = nullptr;
+  int wtype = mhcudaFloat32, ctype = mhcudaUInt32, rtype = mhcudaUInt32;
   uint32_t length = 0;
 };
 
@@ -119,47 +122,64 @@ bool is_csr(PyObject *m) {
   return false;
 }
 
-// A uint32 view of an index array.  Contiguous int32 arrays (scipy's default
-// index type) are used in place: the bits are the same for every valid index,
-// and a negative one reads as a column >= dim, which the device rejects.
-// Other types are cast (a copy), as python.cc:317,323 always does.
-Ref as_u32(PyObject *obj) {
+// An array in a type the engine reads in place, else cast (a copy), as
+// python.cc:310-327 always casts to float32 / uint32.  In place: contiguous,
+// aligned, native-order arrays of float32 (and float64 if `wide`) for data;
+// of int32/uint32 (and int64/uint64 if `wide`) for indices -- the bits of an
+// int32 index equal its uint32 for every valid index, and a negative one
+// reads as a column >= dim, which the device rejects.
+Ref as_engine_array(PyObject *obj, bool floating, bool wide, int *type) {
   if (PyArray_Check(obj)) {
     PyArrayObject *a = reinterpret_cast<PyArrayObject *>(obj);
-    const int t = PyArray_TYPE(a);
-    if ((t == NPY_INT32 || t == NPY_UINT32) && PyArray_ISCARRAY_RO(a) &&
-        PyArray_ISNOTSWAPPED(a)) {
-      Py_INCREF(obj);
-      return Ref(obj);
+    if (PyArray_ISCARRAY_RO(a) && PyArray_ISNOTSWAPPED(a)) {
+      int t = -1;
+      switch (PyArray_TYPE(a)) {
+        case NPY_FLOAT32: t = floating ? mhcudaFloat32 : -1; break;
+        case NPY_FLOAT64: t = floating && wide ? mhcudaFloat64 : -1; break;
+        case NPY_UINT32: t = floating ? -1 : mhcudaUInt32; break;
+        case NPY_INT32: t = floating ? -1 : mhcudaInt32; break;
+        case NPY_INT64: t = !floating && wide ? mhcudaInt64 : -1; break;
+        case NPY_UINT64: t = !floating && wide ? mhcudaUInt64 : -1; break;
+        default: break;
+      }
+      // npy_intp-sized longs alias NPY_INT64 / NPY_UINT64 on LP64.
+      if (t < 0 && !floating && wide && PyArray_ITEMSIZE(a) == 8 && PyArray_ISINTEGER(a))
+        t = PyArray_ISSIGNED(a) ? mhcudaInt64 : mhcudaUInt64;
+      if (t >= 0) {
+        *type = t;
+        Py_INCREF(obj);
+        return Ref(obj);
+      }
     }
   }
-  return Ref(PyArray_FROM_OTF(obj, NPY_UINT32, NPY_ARRAY_FORCECAST | NPY_ARRAY_IN_ARRAY));
+  *type = floating ? mhcudaFloat32 : mhcudaUInt32;
+  return Ref(PyArray_FROM_OTF(obj, floating ? NPY_FLOAT32 : NPY_UINT32,
+                              NPY_ARRAY_FORCECAST | NPY_ARRAY_IN_ARRAY));
 }
 
-bool csr_view(PyObject *m, Csr *out) {
+bool csr_view(PyObject *m, Csr *out, bool wide) {
   if (!is_csr(m)) return false;
   Ref d(PyObject_GetAttrString(m, "data"));
-  if (d)
-    out->data = Ref(PyArray_FROM_OTF(d.get(), NPY_FLOAT32, NPY_ARRAY_FORCECAST | NPY_ARRAY_IN_ARRAY));
+  if (d) out->data = as_engine_array(d.get(), true, wide, &out->wtype);
   if (!out->data) {
     PyErr_SetString(PyExc_ValueError, "Failed to convert csr_matrix.data to numpy.array");
     return false;
   }
   Ref i(PyObject_GetAttrString(m, "indices"));
-  if (i) out->indices = as_u32(i.get());
+  if (i) out->indices = as_engine_array(i.get(), false, wide, &out->ctype);
   if (!out->indices) {
     PyErr_SetString(PyExc_ValueError, "Failed to convert csr_matrix.indices to numpy.array");
     return false;
   }
   Ref p(PyObject_GetAttrString(m, "indptr"));
-  if (p) out->indptr = as_u32(p.get());
+  if (p) out->indptr = as_engine_array(p.get(), false, wide, &out->rtype);
   if (!out->indptr) {
     PyErr_SetString(PyExc_ValueError, "Failed to convert csr_matrix.indptr to numpy.array");
     return false;
   }
-  out->weights = static_cast<const float *>(PyArray_DATA(out->data.arr()));
-  out->cols = static_cast<const uint32_t *>(PyArray_DATA(out->indices.arr()));
-  out->rows = static_cast<const uint32_t *>(PyArray_DATA(out->indptr.arr()));
+  out->weights = PyArray_DATA(out->data.arr());
+  out->cols = PyArray_DATA(out->indices.arr());
+  out->rows = PyArray_DATA(out->indptr.arr());
   const npy_intp n = PyArray_SIZE(out->indptr.arr());
   out->length = n > 0 ? static_cast<uint32_t>(n - 1) : 0;
   return true;
@@ -247,7 +267,7 @@ PyObject *py_calc(PyObject *, PyObject *args, PyObject *kwargs) {
   MinhashCudaGenerator *gen = gen_from(g);
   if (!gen) return nullptr;
   Csr m;
-  if (!csr_view(matrix, &m)) return nullptr;
+  if (!csr_view(matrix, &m, /*wide=*/true)) return nullptr;
   if (row_start >= m.length) {
     PyErr_SetString(PyExc_ValueError,
                     "minhash_cuda_calc: row_start must be less than the total number of rows "
@@ -266,12 +286,13 @@ PyObject *py_calc(PyObject *, PyObject *args, PyObject *kwargs) {
   Ref out(PyArray_EMPTY(3, dims, NPY_UINT32, 0));
   if (!out) return nullptr;
   uint32_t *o = static_cast<uint32_t *>(PyArray_DATA(out.arr()));
-  // mhcuda_calc honours rows[0] != 0 as an absolute offset, so a row slice is
-  // a pointer offset into indptr: no rebased copy (python.cc:349-359 copies).
-  const uint32_t *rows = m.rows + row_start;
+  // mhcuda_calc_typed honours rows[0] != 0 as an offset, so a row slice is a
+  // pointer offset into indptr: no rebased copy (python.cc:349-359 copies).
+  const void *rows = static_cast<const char *>(m.rows) +
+                     static_cast<size_t>(row_start) * PyArray_ITEMSIZE(m.indptr.arr());
   MHCUDAResult r;
   Py_BEGIN_ALLOW_THREADS
-  r = mhcuda_calc(gen, m.weights, m.cols, rows, length, o);
+  r = mhcuda_calc_typed(gen, m.weights, m.wtype, m.cols, m.ctype, rows, m.rtype, length, o);
   Py_END_ALLOW_THREADS
   if (!check(r, "minhash_cuda_calc")) return nullptr;
   return out.release();
@@ -296,10 +317,10 @@ PyObject *py_calc_batch(PyObject *, PyObject *args) {
   if (!result) return nullptr;
   for (Py_ssize_t i = 0; i < n; ++i) {
     PyObject *m = PySequence_Fast_GET_ITEM(fast.get(), i);
-    if (!csr_view(m, &mats[i])) return nullptr;
-    w[i] = mats[i].weights;
-    c[i] = mats[i].cols;
-    rw[i] = mats[i].rows;
+    if (!csr_view(m, &mats[i], /*wide=*/false)) return nullptr;
+    w[i] = static_cast<const float *>(mats[i].weights);
+    c[i] = static_cast<const uint32_t *>(mats[i].cols);
+    rw[i] = static_cast<const uint32_t *>(mats[i].rows);
     len[i] = mats[i].length;
     npy_intp dims[3] = {static_cast<npy_intp>(len[i]), p.samples, 2};
     PyObject *o = PyArray_EMPTY(3, dims, NPY_UINT32, 0);

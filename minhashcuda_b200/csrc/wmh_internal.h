@@ -79,13 +79,13 @@ size_t hash_kernel_registers(uint32_t spl, uint32_t minb);
 
 // Parameter kernels (param_kernels.cu).
 enum class PairOp : int { kGamma = 0, kLogGamma = 1, kCopy = 2 };
-// params[d][which][s] = op(a[s*dim + d], b[s*dim + d]) for s < samples.
+// params[d][which][s_base + s] = op(a[s*dim + d], b[s*dim + d]) for s < samples.
 cudaError_t launch_pack_params(const float *a, const float *b, PairOp op, uint32_t which,
-                               uint32_t dim, uint32_t samples, uint32_t s_pad,
+                               uint32_t dim, uint32_t s_base, uint32_t samples, uint32_t s_pad,
                                float *params, cudaStream_t stream);
-// dst[s*dim + d] = params[d][which][s].
+// dst[s*dim + d] = params[d][which][s_base + s] for s < samples.
 cudaError_t launch_unpack_params(const float *params, uint32_t which, uint32_t dim,
-                                 uint32_t samples, uint32_t s_pad, float *dst,
+                                 uint32_t s_base, uint32_t samples, uint32_t s_pad, float *dst,
                                  cudaStream_t stream);
 cudaError_t launch_logf(const float *in, float *out, size_t n, cudaStream_t stream);
 

@@ -62,7 +62,37 @@ def test_host_side_validation_without_gpu():
     assert lib.mhcuda_retrieve_random_vars(None, None, None, None) == mb.INVALID_ARGUMENTS
     assert lib.mhcuda_assign_random_vars(None, None, None, None) == mb.INVALID_ARGUMENTS
     assert lib.mhcuda_calc_batch(None, 0, None, None, None, None, None) == mb.INVALID_ARGUMENTS
+    assert lib.mhcuda_calc_typed(None, one.ctypes.data, mb.FLOAT64, one.ctypes.data, mb.INT64,
+                                 one.ctypes.data, mb.INT64, 1, one.ctypes.data) == \
+        mb.INVALID_ARGUMENTS
     assert lib.mhcuda_fini(None) == mb.SUCCESS
+
+
+def test_typed_calc_rejects_bad_types_and_offsets_before_device_work():
+    """Element types and 64-bit offsets are checked on the host before the
+    generator is touched, so a dummy non-null handle is never dereferenced."""
+    lib = mb.capi()
+    w = np.ones(4, np.float64)
+    c = np.zeros(4, np.int64)
+    out = np.zeros(64, np.uint32)
+    dummy = ctypes.c_void_p(1)
+
+    def calc(wt, ct, rows, rt):
+        return lib.mhcuda_calc_typed(dummy, w.ctypes.data, wt, c.ctypes.data, ct,
+                                     rows.ctypes.data, rt, len(rows) - 1, out.ctypes.data)
+
+    ok_rows = np.array([0, 2, 4], np.int64)
+    assert calc(mb.UINT32, mb.INT64, ok_rows, mb.INT64) == mb.INVALID_ARGUMENTS  # int weights
+    assert calc(mb.FLOAT64, mb.FLOAT32, ok_rows, mb.INT64) == mb.INVALID_ARGUMENTS  # float cols
+    assert calc(mb.FLOAT64, mb.INT64, ok_rows, 17) == mb.INVALID_ARGUMENTS
+    assert calc(mb.FLOAT64, mb.INT64, np.array([0, 3, 2], np.int64),
+                mb.INT64) == mb.INVALID_ARGUMENTS  # decreasing
+    assert calc(mb.FLOAT64, mb.INT64, np.array([-1, 2, 4], np.int64),
+                mb.INT64) == mb.INVALID_ARGUMENTS  # negative
+    assert calc(mb.FLOAT64, mb.INT64, np.array([0, 2, 1 << 32], np.int64),
+                mb.INT64) == mb.INVALID_ARGUMENTS  # spans 2^32
+    assert calc(mb.FLOAT64, mb.INT64, np.array([0, 2, 1 << 32], np.uint64),
+                mb.UINT64) == mb.INVALID_ARGUMENTS
 
 
 @pytest.mark.skipif(os.path.exists("/dev/nvidia0"), reason="a GPU is present")

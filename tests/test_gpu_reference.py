@@ -105,6 +105,94 @@ def test_curand_parameter_parity(dim, samples, seed):
         np.testing.assert_array_equal(g.view(np.uint32), w.view(np.uint32), err_msg=name)
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("chunk_rows", [1, 3, 8, 37])
+@pytest.mark.parametrize("dim,samples,seed", [(777, 256, 42), (130, 128, 1)])
+def test_curand_parameter_parity_chunked(dim, samples, seed, chunk_rows, monkeypatch):
+    """The table is built a block of sample rows at a time from two
+    generators positioned at absolute offsets; any block size (ragged last
+    blocks, odd dims) gives the reference's single-call draws bit for bit,
+    and retrieve/assign in blocks round-trip."""
+    with _ref_gen(dim, samples, seed=seed) as ref:
+        want = ref.retrieve()
+    monkeypatch.setenv("MHCUDA_B200_PARAM_CHUNK_ROWS", str(chunk_rows))
+    with engine_gen(dim, samples, seed=seed) as eng:
+        got = eng.retrieve()
+    for name, g, w in zip(("rs", "ln_cs", "betas"), got, want):
+        np.testing.assert_array_equal(g.view(np.uint32), w.view(np.uint32), err_msg=name)
+    rng = np.random.default_rng(chunk_rows)
+    mine = [rng.standard_normal((samples, dim)).astype(np.float32) for _ in range(3)]
+    with engine_gen(dim, samples, deferred=True) as eng:
+        eng.assign(*mine)
+        monkeypatch.setenv("MHCUDA_B200_PARAM_CHUNK_ROWS", str(chunk_rows + 5))
+        back = eng.retrieve()
+    for g, w in zip(back, mine):
+        np.testing.assert_array_equal(g, w)
+
+
+@pytest.mark.gpu
+def test_curand_parameter_parity_default_blocks():
+    """3*2^20 dims x 128 samples: 12 MiB per sample row, so the default
+    1 GiB blocks split every run into blocks of 80 and 48 sample rows."""
+    dim, samples, seed = 3 << 20, 128, 9
+    with _ref_gen(dim, samples, seed=seed) as ref:
+        want = ref.retrieve()
+    with engine_gen(dim, samples, seed=seed) as eng:
+        got = eng.retrieve()
+    for name, g, w in zip(("rs", "ln_cs", "betas"), got, want):
+        assert np.array_equal(g.view(np.uint32), w.view(np.uint32)), name
+
+
+def _init_peak(dim, samples, seed, make):
+    """Wall time of one generator init (after a warm-up init of the same
+    shape) and the most device memory in use above the starting level while
+    it ran, sampled from a second thread."""
+    import threading
+    import time
+    import torch
+    make(dim, samples, seed).__exit__(None, None, None)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    low = [free0]
+    stop = threading.Event()
+
+    def poll():
+        while not stop.is_set():
+            low[0] = min(low[0], torch.cuda.mem_get_info()[0])
+            time.sleep(0.0005)
+
+    th = threading.Thread(target=poll)
+    th.start()
+    t0 = time.perf_counter()
+    g = make(dim, samples, seed)
+    t = time.perf_counter() - t0
+    stop.set()
+    th.join()
+    g.__exit__(None, None, None)
+    return t, free0 - low[0]
+
+
+@pytest.mark.gpu
+def test_param_init_scratch_and_time():
+    """Init builds the table a block of sample rows at a time: device memory
+    above the table stays near two 1 GiB blocks (plus cuRAND state) even for
+    2^24 x 256 (a 51.5 GB table, dim*samples = 2^32, which the reference
+    cannot hold), where whole runs would take 2 x 17 GB.  12M x 128 is also
+    timed on the reference build (three full [samples][dim] arrays)."""
+    rec = {"test": "param_init"}
+    eng = lambda d, s, seed: engine_gen(d, s, seed=seed)  # noqa: E731
+    for dim, samples in [(12_000_000, 128), (1 << 24, 256)]:
+        table = dim * 3 * ((samples + 3) // 4 * 4) * 4
+        t, peak = _init_peak(dim, samples, 5, eng)
+        rec[f"engine_{dim}x{samples}"] = {"s": t, "peak_bytes": peak, "table_bytes": table,
+                                          "above_table_bytes": peak - table}
+        assert peak - table < (4 << 30), (peak, table)
+    ref = lambda d, s, seed: _ref_gen(d, s, seed=seed)  # noqa: E731
+    t, peak = _init_peak(12_000_000, 128, 5, ref)
+    rec["reference_12000000x128"] = {"s": t, "peak_bytes": peak}
+    _record(rec)
+
+
 def _compare_with_reference(m, samples, params=None, seed=1):
     dim = m.shape[1]
     with _ref_gen(dim, samples, seed=seed, deferred=params is not None) as ref:
