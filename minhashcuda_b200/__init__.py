@@ -9,7 +9,7 @@ Two ways in, both over the same native library:
   ``include/minhashcuda.h`` and ``include/minhashcuda_b200.h``.
 
 There is no fallback: if the native libraries are missing the import fails.
-Build them with ``python -m minhashcuda_b200._build``.
+Build them with ``python minhashcuda_b200/_build.py``.
 """
 from __future__ import annotations
 
@@ -24,7 +24,7 @@ SYNTH_PATH = os.path.join(HERE, "libmhsynth.so")
 if not os.path.exists(LIB_PATH):
     raise ImportError(
         f"minhashcuda_b200: native library {LIB_PATH} is missing; "
-        "build it with `python -m minhashcuda_b200._build`")
+        "build it with `python minhashcuda_b200/_build.py`")
 
 from . import libMHCUDA  # noqa: E402  (the CPython extension next to this file)
 

@@ -10,7 +10,8 @@ Produces, next to this file:
   libmhsynth.so                          synthetic CSR generators used by the
                                          benchmark and the tests
 
-Run ``python -m minhashcuda_b200._build`` or call ``build()``.
+Run ``python minhashcuda_b200/_build.py`` (by path: importing the package
+needs the libraries this builds) or ``__graft_entry__.build()``.
 """
 from __future__ import annotations
 
