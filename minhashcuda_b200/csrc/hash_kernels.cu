@@ -271,22 +271,114 @@ struct Params {
   }
 };
 
+// ---- Packed pairs of float32 (sm_100 f32x2 arithmetic) --------------------
+// One add/sub/mul/fma.rn.f32x2 applies the IEEE round-to-nearest operation
+// to both halves independently, so a pair computes exactly what two
+// __fadd_rn / __fsub_rn / __fmul_rn / __fmaf_rn calls compute, in one issue.
+struct F2 {
+  unsigned long long v;
+};
+__device__ __forceinline__ F2 f2(float lo, float hi) {
+  F2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void split(F2 x, float &lo, float &hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(x.v));
+}
+__device__ __forceinline__ F2 add2(F2 a, F2 b) {
+  F2 r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ F2 sub2(F2 a, F2 b) {
+  F2 r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ F2 mul2(F2 a, F2 b) {
+  F2 r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ F2 fma2(F2 a, F2 b, F2 c) {
+  F2 r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r.v) : "l"(a.v), "l"(b.v), "l"(c.v));
+  return r;
+}
+
+// Selects for samples j and j+1 given their ln_a pair.
+template <int SPL>
+__device__ __forceinline__ void update_pair(F2 ln_a, float t0, float t1, uint32_t d, int j,
+                                            RowState<SPL> &st) {
+  float l0, l1;
+  split(ln_a, l0, l1);
+  const bool lt0 = l0 < st.mn[j], lt1 = l1 < st.mn[j + 1];
+  st.mn[j] = lt0 ? l0 : st.mn[j];
+  st.kk[j] = lt0 ? d : st.kk[j];
+  st.tf[j] = lt0 ? t0 : st.tf[j];
+  st.mn[j + 1] = lt1 ? l1 : st.mn[j + 1];
+  st.kk[j + 1] = lt1 ? d : st.kk[j + 1];
+  st.tf[j + 1] = lt1 ? t1 : st.tf[j + 1];
+}
+
 template <int SPL>
 __device__ __forceinline__ void eval_all(const Params<SPL> &p, float w, uint32_t d, bool active,
                                          RowState<SPL> &st) {
   float t[SPL];
   bool undecided = false;
+  if constexpr (SPL % 2 == 0) {
+    // fast_t on sample pairs.  The bound is fast_t's; the limit 0.5 - m is
+    // one fma, (|qa| + |b|) * -2^-18 + (0.5 - 2^-18), whose single rounding
+    // (<= 2^-26) is covered by the additive 2^-18 in m.
+    const F2 ww = f2(w, w);
 #pragma unroll
-  for (int j = 0; j < SPL; ++j) undecided |= !fast_t(w, p.r.v[j], p.b.v[j], t[j]);
+    for (int j = 0; j < SPL; j += 2) {
+      float y0, y1;
+      asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y0) : "f"(p.r.v[j]));
+      asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y1) : "f"(p.r.v[j + 1]));
+      const F2 qa = mul2(ww, f2(y0, y1));
+      const F2 va = add2(qa, f2(p.b.v[j], p.b.v[j + 1]));
+      float v0, v1, q0, q1;
+      split(va, v0, v1);
+      split(qa, q0, q1);
+      t[j] = floorf(v0);
+      t[j + 1] = floorf(v1);
+      const F2 fr = sub2(va, f2(t[j], t[j + 1]));
+      const F2 s = f2(__fadd_rn(fabsf(q0), fabsf(p.b.v[j])),
+                      __fadd_rn(fabsf(q1), fabsf(p.b.v[j + 1])));
+      const F2 lim = fma2(s, f2(-kTMargin, -kTMargin), f2(0.5f - kTMargin, 0.5f - kTMargin));
+      const F2 dv = sub2(fr, f2(0.5f, 0.5f));
+      float d0, d1, l0, l1;
+      split(dv, d0, d1);
+      split(lim, l0, l1);
+      undecided |= !(fabsf(d0) < l0) || !(fabsf(d1) < l1);  // NaN -> undecided
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < SPL; ++j) undecided |= !fast_t(w, p.r.v[j], p.b.v[j], t[j]);
+  }
   // Rare: some lane's t sits within the margin of an integer; the warp takes
   // the exact quotient for all its samples (warp-uniform branch).
   if (__any_sync(0xFFFFFFFFu, undecided && active)) {
 #pragma unroll
     for (int j = 0; j < SPL; ++j) t[j] = exact_t(w, p.r.v[j], p.b.v[j]);
   }
+  if constexpr (SPL % 2 == 0) {
+    // ln_a = fma(-(t - beta), r, ln_c) - r on pairs; beta - t is -(t - beta)
+    // exactly (round-to-nearest is symmetric).
 #pragma unroll
-  for (int j = 0; j < SPL; ++j)
-    wmh_update(t[j], p.r.v[j], p.c.v[j], p.b.v[j], d, st.mn[j], st.kk[j], st.tf[j]);
+    for (int j = 0; j < SPL; j += 2) {
+      const F2 rr = f2(p.r.v[j], p.r.v[j + 1]);
+      const F2 nb = sub2(f2(p.b.v[j], p.b.v[j + 1]), f2(t[j], t[j + 1]));
+      const F2 ln_a = sub2(fma2(nb, rr, f2(p.c.v[j], p.c.v[j + 1])), rr);
+      update_pair<SPL>(ln_a, t[j], t[j + 1], d, j, st);
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < SPL; ++j)
+      wmh_update(t[j], p.r.v[j], p.c.v[j], p.b.v[j], d, st.mn[j], st.kk[j], st.tf[j]);
+  }
 }
 
 template <int SPL, int MINB>
