@@ -463,6 +463,40 @@ def run_streamed(args, rank, world, local):
         print(json.dumps(line), flush=True)
 
 
+def srpt_ideal(sizes, rate, load, seed):
+    """Response-time percentiles (ms) of an ideal preemptive
+    shortest-remaining-work-first server of `rate` evals/s, zero overheads,
+    Poisson arrivals at `load` * rate, request sizes `sizes` (evals): a lower
+    bound for any work-conserving scheduler of these requests at that rate."""
+    import heapq
+    rng = np.random.default_rng(seed)
+    sizes = np.asarray(sizes, dtype=np.float64)
+    n = len(sizes)
+    lam = load * rate / sizes.mean()
+    arr = np.cumsum(rng.exponential(1.0 / lam, n))
+    t, heap, resp, i = 0.0, [], np.zeros(n), 0
+    while i < n or heap:
+        if not heap:
+            t = max(t, arr[i])
+            heapq.heappush(heap, (sizes[i] / rate, i))
+            i += 1
+            continue
+        rem, j = heap[0]
+        nxt = arr[i] if i < n else np.inf
+        if t + rem <= nxt:
+            t += rem
+            heapq.heappop(heap)
+            resp[j] = t - arr[j]
+        else:
+            heapq.heapreplace(heap, (rem - (nxt - t), j))
+            t = nxt
+            heapq.heappush(heap, (sizes[i] / rate, i))
+            i += 1
+    r = resp[n // 10:] * 1e3  # skip the warm-up tenth
+    p50, p99, p999 = np.percentile(r, [50, 99, 99.9])
+    return {"p50_ms": float(p50), "p99_ms": float(p99), "p999_ms": float(p999)}
+
+
 def run_serving(args, rank, world, local):
     """Serving: Poisson-arriving requests over three resident generators
     (2^20 dims / 128 samples, 2^22 / 64, 2^24 / 256; 1.6 + 3.2 + 51.5 GB of
@@ -562,7 +596,8 @@ def run_serving(args, rank, world, local):
     peak_reqs = [make_req() for _ in range(400)]
     peak_t = run_closed(peak_reqs)
     peak = sum(r[3] for r in peak_reqs) / peak_t
-    mean_evals = float(np.mean([make_req()[3] for _ in range(20000)]))
+    size_sample = [make_req()[3] for _ in range(40000)]
+    mean_evals = float(np.mean(size_sample))
     log(f"serving: saturated throughput {peak:.3e} evals/s over 400 requests")
 
     levels = []
@@ -607,7 +642,8 @@ def run_serving(args, rank, world, local):
         levels.append({"load": frac, "offered_evals_per_s": lam * mean_evals,
                        "requests": len(reqs), "evals_per_s": done_evals[0] / elapsed,
                        "p50_ms": float(np.percentile(a, 50)), "p99_ms": float(np.percentile(a, 99)),
-                       "p999_ms": float(np.percentile(a, 99.9)), "max_ms": float(a[-1])})
+                       "p999_ms": float(np.percentile(a, 99.9)), "max_ms": float(a[-1]),
+                       "srpt_ideal_at_saturated_rate": srpt_ideal(size_sample, peak, frac, 5)})
         log(f"serving: load {frac:.2f}: {levels[-1]}")
 
     # Each served result equals the same request hashed alone.
@@ -636,7 +672,9 @@ def run_serving(args, rank, world, local):
                                "log-uniform 1..50000 rows, row nnz 50*(1+Zipf(2)), Poisson arrivals",
                    "lanes": args.serving_lanes, "hbm_budget_gib": args.serving_budget,
                    "seconds_per_level": args.serving_seconds},
-        "saturated_evals_per_s": peak, "mean_evals_per_request": mean_evals, "levels": levels,
+        "saturated_evals_per_s": peak, "mean_evals_per_request": mean_evals,
+        "request_evals_p50_p99": [float(x) for x in np.percentile(size_sample, [50, 99])],
+        "levels": levels,
         "bit_exact_served_vs_alone": exact,
     }
     print(json.dumps(line), flush=True)

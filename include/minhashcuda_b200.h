@@ -163,14 +163,17 @@ enum MHCUDAResult mhcuda_jaccard(const MinhashCudaGenerator *gen, const uint32_t
 
 /* ---- Serving: a continuous-batching request loop on one device ----------
  * No counterpart in the reference (every mhcuda_calc there is one blocking
- * launch per device, minhashcuda.cc:583-642).  A worker thread keeps `lanes`
- * batches in flight on separate streams; each request (a CSR and an output
+ * launch per device, minhashcuda.cc:583-642).  `lanes` worker threads keep
+ * batches in flight on their own streams; each request (a CSR and an output
  * buffer in host memory, as for mhcuda_calc, hashed against any generator on
- * the server's device) is cut into row blocks that fit a lane, and free lanes
- * take the oldest waiting blocks of one generator at a time.  Requests that
- * arrive while others run start as soon as a lane frees up.  Device memory
- * used by the server is `hbm_budget_bytes` (split between the lanes at start;
- * nothing grows later).  Results are bit-identical to mhcuda_calc. */
+ * the server's device) is scheduled shortest-remaining-work first: a free
+ * lane batches the requests of one generator with the least work left, whole
+ * where they fit and in row blocks otherwise.  Small batches run on a
+ * high-priority stream straight from mapped host memory; at most lanes - 2
+ * large batches are out at once.  Requests that arrive while others run join
+ * the next batch a lane forms.  Device memory used by the server is
+ * `hbm_budget_bytes` (split between the lanes at start; nothing grows later).
+ * Results are bit-identical to mhcuda_calc. */
 typedef struct MinhashCudaServer_ MinhashCudaServer;
 
 /* Starts a server on the device selected like mhcuda_init's `devices`.

@@ -251,6 +251,9 @@ __device__ __forceinline__ bool finish_window(const HashArgs &a, WarpStage &st, 
     float x;
     if (i < nb) {
       x = st.w[b][i];
+    } else if (a.host_csr) {  // mapped host memory: plain loads
+      x = a.weights[ws + i];
+      st.c[b][i] = a.cols[ws + i];
     } else {
       x = __ldg(a.weights + ws + i);
       st.c[b][i] = __ldg(a.cols + ws + i);
@@ -400,8 +403,9 @@ __global__ void __launch_bounds__(kHashBlock, MINB) hash_kernel(const HashArgs a
   const uint32_t base = a.indptr[0];
   const uint32_t items = a.nchunks * a.ntiles;
   const size_t col_stride = static_cast<size_t>(3) * a.s_pad;
-  const bool bulk_ok = ((reinterpret_cast<uintptr_t>(a.weights) |
-                         reinterpret_cast<uintptr_t>(a.cols)) & 15u) == 0;
+  // Bulk copies only from device memory; mapped host CSR is read by the lanes.
+  const bool bulk_ok = !a.host_csr && ((reinterpret_cast<uintptr_t>(a.weights) |
+                                        reinterpret_cast<uintptr_t>(a.cols)) & 15u) == 0;
 
   for (uint32_t item = gw; item < items; item += nw) {
     const uint32_t c = item / a.ntiles;

@@ -2,17 +2,26 @@
 //
 // The reference has no server: every mhcuda_calc call is one synchronous
 // launch per device (minhashcuda.cc:583-642).  Here several "lanes" share one
-// device.  Each lane is a host thread with its own CUDA stream, device buffers
-// for one batch (CSR in, hashes out, chunk scratch) and pinned host staging.
-// Active requests sit in a round-robin ring.  A free lane walks the ring and
-// takes the next row block ("unit", at most max_unit_evals nnz*samples) of
-// every request of one generator in turn until its batch is full, gathers
-// them into one CSR, runs copy-in, the plan/hash/finalize kernels and
-// copy-out on its stream, waits for its own event and hands the hashes back.
-// Requests that arrive while batches are on the GPU join the ring at once and
-// get their first unit into the next batch any lane forms, so the device is
-// shared between requests (small ones finish quickly, large ones progress
-// block by block) and lanes overlap each other's copies and kernels.  Device
+// device.  Each lane is a host thread with two CUDA streams (high and low
+// priority), device buffers for one batch (CSR in, hashes out, chunk
+// scratch) and pinned host staging.  Active requests wait in a pool.  A free
+// lane forms a batch shortest-remaining-work first: it takes the request with
+// the least work left, then the next smallest of the same generator, each
+// whole while the batch budget (max_batch_evals nnz*samples) lasts; the
+// request that does not fit whole gives a row block and ends the batch.  The
+// batch is gathered into one CSR and copy-in, the plan/hash/finalize kernels
+// and copy-out run on one of the lane's streams; the lane waits for its own
+// event and hands the hashes back.  Requests that arrive while batches are on
+// the GPU join the pool at once and go into the next batch any lane forms.
+// A batch that finishes all of its requests within max_unit_evals is small:
+// it runs on the high-priority stream and uses no copy engine -- the kernels
+// read its CSR from the lane's mapped page-locked staging and write the
+// hashes into mapped host memory, so it never queues behind a large batch's
+// copies.  Large batches launch one chunk per warp (non-persistent), so the
+// blocks of a small batch's kernels are scheduled as soon as blocks of a
+// large one retire instead of after its whole launch, and at most
+// lanes - 2 large batches are out at once, so two lanes are always free for
+// small requests.  Lanes overlap each other's copies and kernels.  Device
 // memory is bounded by the budget given at start: the lanes are sized from
 // it once and nothing grows afterwards.
 //
@@ -67,16 +76,22 @@ struct Unit {
 };
 
 struct Lane {
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;     // low priority
+  cudaStream_t hi = nullptr;         // high priority
+  bool high = false;                 // the current batch runs on `hi`
   cudaEvent_t done_ev = nullptr;
   // device
   float *w = nullptr;
   uint32_t *c = nullptr, *ip = nullptr, *out = nullptr, *chunk_row = nullptr, *status = nullptr;
   float *part_ln = nullptr;
   uint2 *part_kt = nullptr;
-  // pinned host
+  // pinned host, mapped into the device's address space
   float *hw = nullptr;
   uint32_t *hc = nullptr, *hip = nullptr, *hout = nullptr, *hstatus = nullptr;
+  // device addresses of the mapped staging (zero-copy batches)
+  float *mw = nullptr;
+  uint32_t *mc = nullptr, *mip = nullptr, *mout = nullptr, *mstatus = nullptr;
+  bool zero_copy = false;
   std::vector<Unit> units;
   std::vector<uint64_t> unit_rows;  // row offset of each unit inside the batch
   std::vector<uint8_t> unit_direct; // hashes already copied straight to the caller
@@ -101,12 +116,14 @@ struct MinhashCudaServer_ {
   // Per-lane capacities (bytes).
   size_t in_cap = 0, out_cap = 0, scratch_cap = 0;
   size_t scratch_unit = 0;  // scratch = chunk_row (1 unit) | part_ln (4) | part_kt (8)
-  uint64_t max_unit_evals = 128ull << 20;   // nnz*samples of one row block
-  uint64_t max_batch_evals = 1024ull << 20; // nnz*samples of one lane batch
+  uint64_t max_unit_evals = 128ull << 20;   // nnz*samples: high-priority batch limit
+  uint64_t max_batch_evals = 512ull << 20;  // nnz*samples of one lane batch
+  uint32_t max_low_inflight = 6;            // low-priority batches out at once (lanes - 2)
+  uint32_t low_inflight = 0;
   std::vector<Lane> lanes;
 
   std::mutex mu;
-  std::condition_variable work;      // lanes: a request joined the ring (or stop)
+  std::condition_variable work;      // lanes: a request joined the pool (or stop)
   std::condition_variable finished;  // waiters: a request completed
   std::deque<Request *> ring;        // requests with rows not yet handed out
   std::unordered_map<uint64_t, std::unique_ptr<Request>> requests;
@@ -145,6 +162,13 @@ bool is_pinned(const void *p) {
 // Units at least this large move between page-locked caller memory and the
 // device with their own copies instead of through the lane's staging.
 constexpr size_t kDirectCopyBytes = static_cast<size_t>(1) << 20;
+
+// Copies the batch's device status word to the lane's mapped host word and
+// clears it for the next batch (no copy engine involved).
+__global__ void publish_status(uint32_t *d_status, uint32_t *h_status) {
+  *h_status = *d_status;
+  *d_status = 0;
+}
 
 void par_copy(void *dst, const void *src, size_t bytes) {
   const size_t kSplit = static_cast<size_t>(16) << 20;
@@ -190,8 +214,10 @@ MinhashCudaServer_::~MinhashCudaServer_() {
     cudaFreeHost(l.hip);
     cudaFreeHost(l.hout);
     cudaFreeHost(l.hstatus);
+    if (l.hi) cudaStreamSynchronize(l.hi);
     if (l.done_ev) cudaEventDestroy(l.done_ev);
     if (l.stream) cudaStreamDestroy(l.stream);
+    if (l.hi) cudaStreamDestroy(l.hi);
   }
 }
 
@@ -210,7 +236,8 @@ MHCUDAResult MinhashCudaServer_::run_units(Lane &lane, const std::vector<Unit> &
     lane.unit_rows[k + 1] = R;
     pos[k + 1] = N;
   }
-  const cudaStream_t st = lane.stream;
+  const bool high = lane.high && !solo;
+  const cudaStream_t st = high ? lane.hi : lane.stream;
   cudaError_t e = cudaSuccess;
   // Staged units are gathered into contiguous runs of the staging buffers;
   // each run goes over in one copy.  Large page-locked units copy directly.
@@ -225,11 +252,15 @@ MHCUDAResult MinhashCudaServer_::run_units(Lane &lane, const std::vector<Unit> &
     }
     run_begin = run_end;
   };
+  // High-priority batches of a lane with mapped staging use no copy engine:
+  // the kernels read the CSR from the staging and write the hashes into
+  // mapped host memory, so they never queue behind large batches' copies.
+  const bool zc = high && lane.zero_copy;
   for (size_t k = 0; k < units.size(); ++k) {
     const Unit &u = units[k];
     const uint32_t b = u.req->rows[u.r0];
     const uint64_t n = pos[k + 1] - pos[k];
-    if (u.req->in_pinned && n * 4 >= kDirectCopyBytes) {
+    if (!zc && u.req->in_pinned && n * 4 >= kDirectCopyBytes) {
       flush_run();
       if (e == cudaSuccess)
         e = cudaMemcpyAsync(lane.w + pos[k], u.req->weights + b, n * 4, cudaMemcpyHostToDevice, st);
@@ -244,10 +275,23 @@ MHCUDAResult MinhashCudaServer_::run_units(Lane &lane, const std::vector<Unit> &
     uint32_t *ip = lane.hip + lane.unit_rows[k];
     for (uint32_t x = u.r0; x < u.r1; ++x) ip[x - u.r0] = static_cast<uint32_t>(pos[k] + (u.req->rows[x] - b));
   }
-  flush_run();
+  if (!zc) flush_run();
   lane.hip[R] = static_cast<uint32_t>(N);
   const uint32_t s_pad = g.s_pad;
   mhb::HashPlan plan = mhb::plan_for_generator(units.front().req->gen, N, R);
+  const int bps = mhb::hash_blocks_per_sm(plan.spl, plan.minb);
+  // Batches are small next to a plain call: cut at least two waves of warp
+  // items even when rows are long (the plain plan keeps a few rows per chunk).
+  {
+    const uint64_t resident_warps =
+        static_cast<uint64_t>(sm_count) * bps * (mhb::kHashBlock / 32);
+    uint64_t chunk = (N * plan.ntiles + 2 * resident_warps - 1) / (2 * resident_warps);
+    chunk = std::max<uint64_t>(64, (chunk + 31) & ~31ull);
+    if (chunk < plan.chunk) {
+      plan.chunk = static_cast<uint32_t>(chunk);
+      plan.nchunks = static_cast<uint32_t>(N == 0 ? 1 : (N + chunk - 1) / chunk);
+    }
+  }
   // Keep the chunk table and partials inside the lane's fixed scratch:
   // nchunks*4 <= unit, 2*nchunks*s_pad*4 <= 4*unit, 2*nchunks*s_pad*8 <= 8*unit.
   const uint64_t max_chunks = std::max<uint64_t>(
@@ -257,19 +301,25 @@ MHCUDAResult MinhashCudaServer_::run_units(Lane &lane, const std::vector<Unit> &
     chunk = (chunk + 31) & ~31ull;
     plan.chunk = static_cast<uint32_t>(chunk);
     plan.nchunks = static_cast<uint32_t>((N + chunk - 1) / chunk);
+  }
+  // High priority: a persistent grid.  Low priority: one item per warp, so
+  // blocks retire often and high-priority blocks get their SMs.
+  {
     const uint64_t items = static_cast<uint64_t>(plan.nchunks) * plan.ntiles;
-    const int bps = mhb::hash_blocks_per_sm(plan.spl, plan.minb);
+    const uint64_t blocks = (items + 7) / 8;
+    const uint64_t resident = static_cast<uint64_t>(sm_count) * bps;
     plan.grid = static_cast<uint32_t>(std::max<uint64_t>(
-        1, std::min<uint64_t>((items + 7) / 8, static_cast<uint64_t>(sm_count) * bps)));
+        1, high ? std::min(blocks, resident) : std::min<uint64_t>(blocks, 1u << 30)));
   }
   mhb::HashArgs a{};
   a.params = g.params;
   a.dim = g.dim;
   a.samples = g.samples;
   a.s_pad = s_pad;
-  a.weights = lane.w;
-  a.cols = lane.c;
-  a.indptr = lane.ip;
+  a.weights = zc ? lane.mw : lane.w;
+  a.cols = zc ? lane.mc : lane.c;
+  a.indptr = zc ? lane.mip : lane.ip;
+  a.host_csr = zc ? 1u : 0u;
   a.rows = static_cast<uint32_t>(R);
   a.nnz = static_cast<uint32_t>(N);
   a.chunk = plan.chunk;
@@ -278,17 +328,22 @@ MHCUDAResult MinhashCudaServer_::run_units(Lane &lane, const std::vector<Unit> &
   a.chunk_row = lane.chunk_row;
   a.part_ln = lane.part_ln;
   a.part_kt = lane.part_kt;
-  a.out = lane.out;
-  a.status = lane.status;
-  if (e == cudaSuccess) e = cudaMemcpyAsync(lane.ip, lane.hip, (R + 1) * 4, cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess) e = cudaMemsetAsync(lane.status, 0, 4, st);
+  a.out = zc ? lane.mout : lane.out;
+  a.status = lane.status;  // zero between batches: publish_status clears it
+  if (e == cudaSuccess && !zc)
+    e = cudaMemcpyAsync(lane.ip, lane.hip, (R + 1) * 4, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = mhb::launch_plan(a, st);
   if (e == cudaSuccess) e = mhb::launch_hash(a, plan, st);
   if (e == cudaSuccess && plan.nchunks > 1) e = mhb::launch_finalize(a, st);
+  if (e == cudaSuccess) {
+    publish_status<<<1, 1, 0, st>>>(lane.status, lane.mstatus);
+    e = cudaGetLastError();
+  }
   // Hashes: large units into page-locked outputs directly, the rest through
-  // the lane's staging (copied out by complete()).
+  // the lane's staging (copied out by complete()); zero-copy batches have
+  // theirs in the staging already.
   lane.unit_direct.assign(units.size(), 0);
-  for (size_t k = 0; k < units.size() && e == cudaSuccess; ++k) {
+  for (size_t k = 0; k < units.size() && e == cudaSuccess && !zc; ++k) {
     const Unit &u = units[k];
     const size_t bytes = unit_out_bytes(u);
     const size_t off = lane.unit_rows[k] * g.samples * 2;
@@ -300,7 +355,6 @@ MHCUDAResult MinhashCudaServer_::run_units(Lane &lane, const std::vector<Unit> &
       e = cudaMemcpyAsync(lane.hout + off, lane.out + off, bytes, cudaMemcpyDeviceToHost, st);
     }
   }
-  if (e == cudaSuccess) e = cudaMemcpyAsync(lane.hstatus, lane.status, 4, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaEventRecord(lane.done_ev, st);
   if (e == cudaSuccess && solo) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
@@ -318,93 +372,83 @@ void MinhashCudaServer_::finish_locked(Request *r, Clock::time_point now) {
     latencies_ms.push_back(std::chrono::duration<double, std::milli>(now - r->submitted).count());
 }
 
-// Under `mu`: fills lane.units by walking the ring from its head, one unit
-// per request of the first request's generator per pass, until the batch is
-// full; requests whose rows are all handed out leave the ring, the others
-// rotate to its back (round-robin).  Returns false if nothing was taken.
+// Under `mu`: fills lane.units shortest-remaining-work first.  Requests are
+// ordered by the nnz*samples they have left; the smallest fixes the batch's
+// generator; requests of that generator join whole while the batch budget and
+// the lane's capacities last, and the first that does not fit whole gives its
+// next row block (at least one row) and ends the batch.  Cancelled requests
+// leave the pool.  Returns false if nothing was taken.
 bool MinhashCudaServer_::take(Lane &lane) {
-  std::vector<Unit> batch;
-  size_t in = 0, out = 0;
-  uint64_t evals = 0;
-  const MinhashCudaGenerator_ *gen = nullptr;
-  // Small-first: a request whose remaining work fits one unit joins this
-  // batch ahead of the round-robin, so short requests never wait behind the
-  // blocks of long ones.
   auto remaining = [](const Request *r) {
     return (static_cast<uint64_t>(r->rows[r->length]) - r->rows[r->next_row]) * r->g.samples;
   };
+  std::vector<std::pair<uint64_t, Request *>> order;
+  order.reserve(ring.size());
   for (auto it = ring.begin(); it != ring.end();) {
     Request *r = *it;
-    if (r->cancelled || remaining(r) > max_unit_evals || (gen && r->gen != gen)) {
-      ++it;
+    if (r->cancelled) {
+      if (r->inflight == 0 && !r->done) finish_locked(r, Clock::now());
+      it = ring.erase(it);
       continue;
     }
-    const size_t ui = static_cast<size_t>(r->rows[r->length] - r->rows[r->next_row]) * 8 +
-                      (static_cast<size_t>(r->length - r->next_row) + 1) * 4;
-    const size_t uo = static_cast<size_t>(r->length - r->next_row) * r->g.samples * 8;
-    if (in + ui > in_cap || out + uo > out_cap || evals + remaining(r) > max_batch_evals) {
-      ++it;
-      continue;
+    order.emplace_back(remaining(r), r);
+    ++it;
+  }
+  // With max_low_inflight low-priority batches out, only requests that fit a
+  // high-priority batch whole are taken: the other lanes stay free for small
+  // requests, whose copies then do not queue behind large ones.
+  const bool allow_low = low_inflight < max_low_inflight;
+  if (!allow_low)
+    order.erase(std::remove_if(order.begin(), order.end(),
+                               [&](const auto &x) { return x.first > max_unit_evals; }),
+                order.end());
+  if (order.empty()) return false;
+  const uint64_t budget = allow_low ? max_batch_evals : max_unit_evals;
+  std::sort(order.begin(), order.end(), [](const auto &x, const auto &y) {
+    return x.first != y.first ? x.first < y.first : x.second->ticket < y.second->ticket;
+  });
+  const MinhashCudaGenerator_ *gen = order.front().second->gen;
+  std::vector<Unit> batch;
+  size_t in = 0, out = 0;
+  uint64_t evals = 0;
+  bool whole = true;
+  for (const auto &entry : order) {
+    Request *r = entry.second;
+    if (r->gen != gen) continue;
+    if (evals >= budget) break;
+    const uint64_t S = r->g.samples;
+    const size_t row_out = S * 8;
+    uint32_t r1 = r->next_row;
+    uint64_t ue = 0;
+    size_t ui = 4, uo = 0;
+    while (r1 < r->length) {
+      const uint64_t nz = static_cast<uint64_t>(r->rows[r1 + 1]) - r->rows[r1];
+      const size_t add_in = nz * 8 + 4;
+      if (in + ui + add_in > in_cap || out + uo + row_out > out_cap) break;
+      if (r1 != r->next_row && evals + ue + nz * S > budget) break;
+      ui += add_in;
+      uo += row_out;
+      ue += nz * S;
+      ++r1;
     }
-    gen = r->gen;
-    evals += remaining(r);
+    if (r1 == r->next_row) continue;  // not even one row fits what is left
+    if (!allow_low && r1 < r->length) break;  // would not finish in this batch
+    batch.push_back(Unit{r, r->next_row, r1});
+    r->next_row = r1;
+    ++r->inflight;
     in += ui;
     out += uo;
-    batch.push_back(Unit{r, r->next_row, r->length});
-    r->next_row = r->length;
-    ++r->inflight;
-    it = ring.erase(it);
-  }
-  bool grew = true;
-  while (grew && !ring.empty()) {
-    grew = false;
-    const size_t n = ring.size();
-    for (size_t k = 0; k < n && !ring.empty(); ++k) {
-      Request *r = ring.front();
-      ring.pop_front();
-      if (r->cancelled) {
-        if (r->inflight == 0 && !r->done) finish_locked(r, Clock::now());
-        continue;
-      }
-      if ((gen && r->gen != gen) || evals >= max_batch_evals) {
-        ring.push_back(r);
-        continue;
-      }
-      // Next row block of r: at least one row, then rows while the unit stays
-      // under max_unit_evals and the batch under the lane's capacities.
-      const uint64_t S = r->g.samples;
-      const size_t row_out = S * 8;
-      uint32_t r1 = r->next_row;
-      uint64_t ue = 0;
-      size_t ui = 4, uo = 0;
-      while (r1 < r->length) {
-        const uint64_t nz = static_cast<uint64_t>(r->rows[r1 + 1]) - r->rows[r1];
-        const size_t add_in = nz * 8 + 4;
-        const bool first = r1 == r->next_row;
-        if (in + ui + add_in > in_cap || out + uo + row_out > out_cap) break;
-        if (!first && (ue + nz * S > max_unit_evals || evals + ue + nz * S > max_batch_evals))
-          break;
-        ui += add_in;
-        uo += row_out;
-        ue += nz * S;
-        ++r1;
-      }
-      if (r1 == r->next_row) {  // does not fit what is left of this batch
-        ring.push_back(r);
-        continue;
-      }
-      gen = r->gen;
-      batch.push_back(Unit{r, r->next_row, r1});
-      r->next_row = r1;
-      ++r->inflight;
-      in += ui;
-      out += uo;
-      evals += ue;
-      grew = true;
-      if (r->next_row < r->length) ring.push_back(r);
+    evals += ue;
+    if (r->next_row < r->length) {
+      whole = false;
+      break;
     }
   }
   if (batch.empty()) return false;
+  for (auto it = ring.begin(); it != ring.end();)
+    it = ((*it)->next_row == (*it)->length) ? ring.erase(it) : std::next(it);
+  lane.high = whole && evals <= max_unit_evals;
+  if (!lane.high) ++low_inflight;
   lane.units = std::move(batch);
   return true;
 }
@@ -434,6 +478,10 @@ void MinhashCudaServer_::complete(Lane &lane, MHCUDAResult launch_result) {
     }
   }
   std::lock_guard<std::mutex> lock(mu);
+  if (!lane.high) {
+    --low_inflight;
+    work.notify_all();
+  }
   const Clock::time_point now = Clock::now();
   for (size_t k = 0; k < units.size(); ++k) {
     Request *r = units[k].req;
@@ -450,10 +498,13 @@ void MinhashCudaServer_::lane_loop(Lane &lane) {
   cudaSetDevice(device);
   for (;;) {
     {
+      // Woken by a submit, a low-priority batch finishing, or stop.
       std::unique_lock<std::mutex> lock(mu);
-      work.wait(lock, [&] { return stop || !ring.empty(); });
-      if (ring.empty()) return;  // stop requested and nothing left
-      if (!take(lane)) continue;
+      for (;;) {
+        if (stop && ring.empty()) return;  // stop requested and nothing left
+        if (take(lane)) break;
+        work.wait(lock);
+      }
     }
     MHCUDAResult r = run_units(lane, lane.units, false);
     if (r == mhcudaSuccess && cudaEventSynchronize(lane.done_ev) != cudaSuccess) {
@@ -495,6 +546,8 @@ MinhashCudaServer *mhcuda_server_start(uint32_t devices, uint64_t hbm_budget_byt
   srv->verbosity = verbosity;
   srv->max_unit_evals = env_u64("MHCUDA_B200_SERVER_UNIT_EVALS", srv->max_unit_evals);
   srv->max_batch_evals = env_u64("MHCUDA_B200_SERVER_BATCH_EVALS", srv->max_batch_evals);
+  srv->max_low_inflight = static_cast<uint32_t>(std::min<uint64_t>(
+      lanes, env_u64("MHCUDA_B200_SERVER_LOW_INFLIGHT", lanes > 2 ? lanes - 2 : 1)));
   cudaDeviceGetAttribute(&srv->sm_count, cudaDevAttrMultiProcessorCount, dev);
   const size_t per_lane = hbm_budget_bytes / lanes;
   srv->in_cap = align256(per_lane * 4 / 10);
@@ -502,20 +555,48 @@ MinhashCudaServer *mhcuda_server_start(uint32_t devices, uint64_t hbm_budget_byt
   srv->scratch_cap = align256(per_lane - srv->in_cap - srv->out_cap);
   srv->scratch_unit = (srv->scratch_cap / 13) & ~static_cast<size_t>(255);
   srv->lanes.resize(lanes);
+  constexpr unsigned kMapped = cudaHostAllocMapped;
+  int can_map = 0;
+  cudaDeviceGetAttribute(&can_map, cudaDevAttrCanMapHostMemory, dev);
+  const bool zero_copy_ok =
+      can_map != 0 && env_u64("MHCUDA_B200_SERVER_NO_ZERO_COPY", 0) == 0;
+  int prio_low = 0, prio_high = 0;  // numerically lower is higher priority
+  if (cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high) != cudaSuccess) {
+    cudaGetLastError();
+    prio_low = prio_high = 0;
+  }
   for (Lane &l : srv->lanes) {
     const size_t max_nnz = srv->in_cap / 8;
-    bool ok = cudaStreamCreateWithFlags(&l.stream, cudaStreamNonBlocking) == cudaSuccess &&
+    bool ok = cudaStreamCreateWithPriority(&l.stream, cudaStreamNonBlocking, prio_low) ==
+                  cudaSuccess &&
+              cudaStreamCreateWithPriority(&l.hi, cudaStreamNonBlocking, prio_high) == cudaSuccess &&
               cudaEventCreateWithFlags(&l.done_ev, cudaEventDisableTiming) == cudaSuccess &&
               cudaMalloc(&l.w, max_nnz * 4 + 16) == cudaSuccess &&
               cudaMalloc(&l.c, max_nnz * 4 + 16) == cudaSuccess &&
               cudaMalloc(&l.ip, srv->in_cap + 256) == cudaSuccess &&
               cudaMalloc(&l.out, srv->out_cap) == cudaSuccess &&
               cudaMalloc(&l.status, 256) == cudaSuccess &&
-              cudaHostAlloc(reinterpret_cast<void **>(&l.hw), max_nnz * 4 + 16, 0) == cudaSuccess &&
-              cudaHostAlloc(reinterpret_cast<void **>(&l.hc), max_nnz * 4 + 16, 0) == cudaSuccess &&
-              cudaHostAlloc(reinterpret_cast<void **>(&l.hip), srv->in_cap + 256, 0) == cudaSuccess &&
-              cudaHostAlloc(reinterpret_cast<void **>(&l.hout), srv->out_cap, 0) == cudaSuccess &&
-              cudaHostAlloc(reinterpret_cast<void **>(&l.hstatus), 256, 0) == cudaSuccess;
+              cudaHostAlloc(reinterpret_cast<void **>(&l.hw), max_nnz * 4 + 16, kMapped) ==
+                  cudaSuccess &&
+              cudaHostAlloc(reinterpret_cast<void **>(&l.hc), max_nnz * 4 + 16, kMapped) ==
+                  cudaSuccess &&
+              cudaHostAlloc(reinterpret_cast<void **>(&l.hip), srv->in_cap + 256, kMapped) ==
+                  cudaSuccess &&
+              cudaHostAlloc(reinterpret_cast<void **>(&l.hout), srv->out_cap, kMapped) ==
+                  cudaSuccess &&
+              cudaHostAlloc(reinterpret_cast<void **>(&l.hstatus), 256, kMapped) == cudaSuccess &&
+              cudaMemset(l.status, 0, 256) == cudaSuccess &&
+              cudaHostGetDevicePointer(reinterpret_cast<void **>(&l.mstatus), l.hstatus, 0) ==
+                  cudaSuccess;
+    // Device addresses of the staging for zero-copy batches; without them a
+    // lane copies every batch.
+    l.zero_copy =
+        ok && zero_copy_ok &&
+        cudaHostGetDevicePointer(reinterpret_cast<void **>(&l.mw), l.hw, 0) == cudaSuccess &&
+        cudaHostGetDevicePointer(reinterpret_cast<void **>(&l.mc), l.hc, 0) == cudaSuccess &&
+        cudaHostGetDevicePointer(reinterpret_cast<void **>(&l.mip), l.hip, 0) == cudaSuccess &&
+        cudaHostGetDevicePointer(reinterpret_cast<void **>(&l.mout), l.hout, 0) == cudaSuccess;
+    if (ok && !l.zero_copy) cudaGetLastError();
     // Scratch: chunk table then partial minima, carved from one allocation.
     char *scratch = nullptr;
     ok = ok && cudaMalloc(&scratch, srv->scratch_cap) == cudaSuccess;

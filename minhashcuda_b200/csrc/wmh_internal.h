@@ -66,6 +66,7 @@ struct HashArgs {
   uint2 *part_kt;            // [2*nchunks][s_pad] partial (k, float bits of t)
   uint32_t *out;             // [rows][samples][2]
   uint32_t *status;          // device status word
+  uint32_t host_csr;         // weights/cols/indptr/out are mapped host memory
 };
 
 // Launchers (hash_kernels.cu).  All enqueue on `stream` and return the launch
