@@ -282,6 +282,14 @@ HashPlan make_plan(const Gen *gen, uint64_t nnz, uint64_t rows, const TuneChoice
   // Rows shorter than a chunk finish inside it; aim for a few rows per chunk.
   const uint64_t avg_row = rows ? (nnz + rows - 1) / rows : 1;
   chunk = std::max<uint64_t>(chunk, std::min<uint64_t>(4 * avg_row, 1024));
+  // Warps take items round-robin (static), so a launch with few items per
+  // warp ends on a ragged last wave: keep at least 8 items per resident warp
+  // even if rows then span chunks (their partials are merged by finalize).
+  {
+    const uint64_t min_items = resident_warps * 8;
+    chunk = std::min<uint64_t>(
+        chunk, std::max<uint64_t>(64, (nnz * p.ntiles + min_items - 1) / min_items));
+  }
   const int forced = env_int("MHCUDA_B200_CHUNK", 0);
   if (forced > 0) chunk = static_cast<uint64_t>(forced);
   chunk = std::max<uint64_t>(64, (chunk + 31) & ~31ull);
@@ -522,15 +530,81 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
     return mhcudaSuccess;
   };
 
+  // Blocks [r0, r1): as many rows as fit the block's nnz (at least one).
+  // Hashing cannot start before the first block has crossed the bus, so the
+  // first block is small -- 16M nnz, still a few waves of warp items -- and
+  // later ones grow geometrically to block_nnz; the factor keeps each block's
+  // copy-in (8 B per nnz) shorter than the previous block's hashing (samples
+  // evals per nnz): about samples / 112 on a B200 with a Gen5 x16 link.
+  // MHCUDA_B200_BLOCK_NNZ gives constant blocks.
+  struct Block {
+    uint32_t r0, r1;
+  };
+  std::vector<Block> blocks;
+  {
+    uint64_t cur = forced > 0 ? block_nnz
+                              : std::min(block_nnz, std::max<uint64_t>(block_nnz / 32, 16ull << 20));
+    const double growth =
+        forced > 0 ? 1.0 : std::min(2.0, std::max(1.15, gen->samples / 112.0));
+    for (uint32_t r0 = 0; r0 < length;) {
+      const uint64_t limit = static_cast<uint64_t>(rows[r0]) + cur;
+      uint32_t r1 = static_cast<uint32_t>(
+          std::upper_bound(rows + r0 + 1, rows + length + 1, limit,
+                           [](uint64_t v, uint32_t x) { return v < x; }) - rows) - 1;
+      r1 = std::max(r1, r0 + 1);
+      blocks.push_back(Block{r0, r1});
+      r0 = r1;
+      cur = std::min<uint64_t>(block_nnz, static_cast<uint64_t>(static_cast<double>(cur) * growth));
+    }
+    // Only the last block's copy-out is left once hashing ends: end on a
+    // small block.
+    const uint64_t tail = std::max<uint64_t>(block_nnz / 16, 1ull << 20);
+    const Block last = blocks.back();
+    if (forced <= 0 && static_cast<uint64_t>(rows[last.r1]) - rows[last.r0] > 2 * tail) {
+      const uint64_t target = static_cast<uint64_t>(rows[last.r1]) - tail;
+      const uint32_t mid = static_cast<uint32_t>(
+          std::upper_bound(rows + last.r0 + 1, rows + last.r1, target,
+                           [](uint64_t v, uint32_t x) { return v < x; }) - rows);
+      if (mid > last.r0 && mid < last.r1) {
+        blocks.back().r1 = mid;
+        blocks.push_back(Block{mid, last.r1});
+      }
+    }
+  }
+  // Size the slots and the launch scratch once for the largest block: growing
+  // a buffer between blocks would free device memory, which waits for all
+  // work in flight and stalls the pipeline.
+  {
+    uint64_t max_n = 0, max_len = 0;
+    uint32_t max_chunks = 1;
+    for (const Block &b : blocks) {
+      const uint64_t n = static_cast<uint64_t>(rows[b.r1]) - rows[b.r0];
+      max_n = std::max(max_n, n);
+      max_len = std::max<uint64_t>(max_len, b.r1 - b.r0);
+      max_chunks = std::max(max_chunks, make_plan(gen, n, b.r1 - b.r0).nchunks);
+    }
+    for (Gen::Slot &sl : gen->slots) {
+      MHB_CHECK(gen, sl.w.ensure(max_n * 4 + 16), mhcudaMemoryAllocationFailure);
+      MHB_CHECK(gen, sl.c.ensure(max_n * 4 + 16), mhcudaMemoryAllocationFailure);
+      MHB_CHECK(gen, sl.ip.ensure((max_len + 1) * 4), mhcudaMemoryAllocationFailure);
+      MHB_CHECK(gen, sl.out.ensure(max_len * row_bytes), mhcudaMemoryAllocationFailure);
+      if (!pin_in) {
+        MHB_CHECK(gen, sl.hw.ensure(max_n * 4), mhcudaMemoryAllocationFailure);
+        MHB_CHECK(gen, sl.hc.ensure(max_n * 4), mhcudaMemoryAllocationFailure);
+        MHB_CHECK(gen, sl.hip.ensure((max_len + 1) * 4), mhcudaMemoryAllocationFailure);
+      }
+      if (!pin_out) MHB_CHECK(gen, sl.hout.ensure(max_len * row_bytes), mhcudaMemoryAllocationFailure);
+    }
+    HashPlan big{};
+    big.nchunks = max_chunks;
+    HashArgs unused{};
+    const MHCUDAResult pr = prepare_launch(gen, 0, 0, big, &unused);
+    if (pr != mhcudaSuccess) return pr;
+  }
+
   MHCUDAResult r = mhcudaSuccess;
-  uint32_t r0 = 0;
-  for (uint32_t i = 0; r0 < length && r == mhcudaSuccess; ++i) {
-    // Block [r0, r1): as many rows as fit in block_nnz (at least one).
-    const uint64_t limit = static_cast<uint64_t>(rows[r0]) + block_nnz;
-    uint32_t r1 = static_cast<uint32_t>(
-        std::upper_bound(rows + r0 + 1, rows + length + 1, limit,
-                         [](uint64_t v, uint32_t x) { return v < x; }) - rows) - 1;
-    r1 = std::max(r1, r0 + 1);
+  for (uint32_t i = 0; i < blocks.size() && r == mhcudaSuccess; ++i) {
+    const uint32_t r0 = blocks[i].r0, r1 = blocks[i].r1;
     Gen::Slot &sl = gen->slots[i & 1];
     r = retire(sl);
     if (r != mhcudaSuccess) break;
@@ -597,7 +671,6 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
     MHB_CHECK(gen, cudaEventRecord(sl.d2h, gen->s_out), mhcudaRuntimeError);
     sl.busy = true;
     MHB_DEBUG(gen, "block %u: rows [%u, %u) nnz %u chunk %u\n", i, r0, r1, n, plan.chunk);
-    r0 = r1;
   }
   for (auto &sl : gen->slots) {
     const MHCUDAResult rr = retire(sl);
