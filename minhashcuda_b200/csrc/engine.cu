@@ -159,7 +159,11 @@ struct MinhashCudaGenerator_ {
     uint32_t *pending_out = nullptr;  // caller destination of a staged block of hashes
     size_t pending_bytes = 0;
   };
-  mutable Slot slots[2];
+  // Pipelines: calc_pipelined uses the first kPipeSlots, mhcuda_calc_batch
+  // all kBatchSlots (its host gather/scatter per group is as long as the
+  // group's device work, so it keeps one more group in flight).
+  static constexpr int kPipeSlots = 2, kBatchSlots = 3;
+  mutable Slot slots[kBatchSlots];
   mutable cudaStream_t s_in = nullptr, s_out = nullptr;
   // Autotuner results by shape class (see tune_key); read by every planner,
   // including the server's lane threads, hence its own lock.
@@ -583,7 +587,8 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
       max_len = std::max<uint64_t>(max_len, b.r1 - b.r0);
       max_chunks = std::max(max_chunks, make_plan(gen, n, b.r1 - b.r0).nchunks);
     }
-    for (Gen::Slot &sl : gen->slots) {
+    for (int k = 0; k < Gen::kPipeSlots; ++k) {
+      Gen::Slot &sl = gen->slots[k];
       MHB_CHECK(gen, sl.w.ensure(max_n * 4 + 16), mhcudaMemoryAllocationFailure);
       MHB_CHECK(gen, sl.c.ensure(max_n * 4 + 16), mhcudaMemoryAllocationFailure);
       MHB_CHECK(gen, sl.ip.ensure((max_len + 1) * 4), mhcudaMemoryAllocationFailure);
@@ -605,7 +610,7 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
   MHCUDAResult r = mhcudaSuccess;
   for (uint32_t i = 0; i < blocks.size() && r == mhcudaSuccess; ++i) {
     const uint32_t r0 = blocks[i].r0, r1 = blocks[i].r1;
-    Gen::Slot &sl = gen->slots[i & 1];
+    Gen::Slot &sl = gen->slots[i % Gen::kPipeSlots];
     r = retire(sl);
     if (r != mhcudaSuccess) break;
     const uint32_t len = r1 - r0;
@@ -1172,7 +1177,11 @@ enum MHCUDAResult mhcuda_calc_batch(const MinhashCudaGenerator *gen, uint32_t co
   MHB_CHECK(gen, batch_streams(gen), mhcudaRuntimeError);
   const cudaStream_t st = gen->stream;
   const size_t row_bytes = static_cast<size_t>(gen->samples) * 2 * sizeof(uint32_t);
+  // Groups grow to group_nnz (MHCUDA_B200_BATCH_GROUP_NNZ); with
+  // MHCUDA_B200_BLOCK_NNZ every group is that size.
   uint64_t group_nnz = 64ull << 20;
+  const int cap = env_int("MHCUDA_B200_BATCH_GROUP_NNZ", 0);
+  if (cap > 0) group_nnz = static_cast<uint64_t>(cap);
   const int forced = env_int("MHCUDA_B200_BLOCK_NNZ", 0);
   if (forced > 0) group_nnz = static_cast<uint64_t>(forced);
   const uint64_t group_rows = 1u << 20;
@@ -1184,7 +1193,7 @@ enum MHCUDAResult mhcuda_calc_batch(const MinhashCudaGenerator *gen, uint32_t co
   struct Pending {
     uint32_t first = 0, last = 0;  // matrices [first, last)
   };
-  Pending pending[2];
+  Pending pending[Gen::kBatchSlots];
   auto retire = [&](uint32_t k) -> MHCUDAResult {
     Gen::Slot &sl = gen->slots[k];
     if (!sl.busy) return mhcudaSuccess;
@@ -1206,32 +1215,87 @@ enum MHCUDAResult mhcuda_calc_batch(const MinhashCudaGenerator *gen, uint32_t co
     return mhcudaSuccess;
   };
 
-  MHCUDAResult r = mhcudaSuccess;
-  uint32_t m0 = 0;
-  for (uint32_t g = 0; m0 < count && r == mhcudaSuccess; ++g) {
-    // Group [m0, m1): consecutive matrices up to ~group_nnz entries / group_rows rows.
-    uint32_t m1 = m0;
-    uint64_t gn = 0, gr = 0;
-    while (m1 < count) {
-      const uint64_t n = nnz_of[m1], l = lengths[m1];
-      if (m1 > m0 && (gn + n > group_nnz || gr + l > group_rows)) break;
-      if (gn + n >= 0xFFFFFFFFull || gr + l >= 0xFFFFFFFFull) {
-        if (m1 == m0) r = mhcudaInvalidArguments;
-        break;
+  // Groups [m0, m1) of consecutive matrices, planned up front: the first is
+  // small (hashing waits for its gather and copy-in) and later ones grow to
+  // group_nnz; the last is split off small (its copy-out and scatter are left
+  // once hashing ends).  MHCUDA_B200_BLOCK_NNZ gives constant groups.
+  struct Group {
+    uint32_t m0, m1;
+    uint64_t nnz, rows;
+  };
+  std::vector<Group> groups;
+  {
+    uint64_t cur = forced > 0 ? group_nnz : std::max<uint64_t>(group_nnz / 8, 1);
+    for (uint32_t m0 = 0; m0 < count;) {
+      uint32_t m1 = m0;
+      uint64_t gn = 0, gr = 0;
+      while (m1 < count) {
+        const uint64_t n = nnz_of[m1], l = lengths[m1];
+        if (m1 > m0 && (gn + n > cur || gr + l > group_rows)) break;
+        if (gn + n >= 0xFFFFFFFFull || gr + l >= 0xFFFFFFFFull) {
+          if (m1 == m0) return mhcudaInvalidArguments;
+          break;
+        }
+        gn += n;
+        gr += l;
+        ++m1;
       }
-      gn += n;
-      gr += l;
-      ++m1;
+      groups.push_back(Group{m0, m1, gn, gr});
+      m0 = m1;
+      if (forced <= 0) cur = std::min(group_nnz, std::max(cur + 1, cur * 3 / 2));
     }
-    if (r != mhcudaSuccess) break;
-    const uint32_t k = g & 1;
+    const uint64_t tail = std::max<uint64_t>(group_nnz / 8, 1);
+    const Group last = groups.back();
+    if (forced <= 0 && last.nnz > 2 * tail && last.m1 - last.m0 > 1) {
+      uint32_t m = last.m1;
+      uint64_t tn = 0, tr = 0;
+      while (m > last.m0 + 1 && tn + nnz_of[m - 1] <= tail) {
+        tn += nnz_of[m - 1];
+        tr += lengths[m - 1];
+        --m;
+      }
+      if (m < last.m1) {
+        groups.back() = Group{last.m0, m, last.nnz - tn, last.rows - tr};
+        groups.push_back(Group{m, last.m1, tn, tr});
+      }
+    }
+  }
+  // Slots and scratch sized once for the largest group (growing a buffer
+  // mid-pipeline frees device memory, which waits for all work in flight).
+  {
+    uint64_t max_n = 0, max_r = 0;
+    uint32_t max_chunks = 1;
+    for (const Group &gp : groups) {
+      max_n = std::max(max_n, gp.nnz);
+      max_r = std::max(max_r, gp.rows);
+      if (gp.rows) max_chunks = std::max(max_chunks, make_plan(gen, gp.nnz, gp.rows).nchunks);
+    }
+    for (Gen::Slot &sl : gen->slots) {
+      MHB_CHECK(gen, sl.hw.ensure(max_n * 4), mhcudaMemoryAllocationFailure);
+      MHB_CHECK(gen, sl.hc.ensure(max_n * 4), mhcudaMemoryAllocationFailure);
+      MHB_CHECK(gen, sl.hip.ensure((max_r + 1) * 4), mhcudaMemoryAllocationFailure);
+      MHB_CHECK(gen, sl.hout.ensure(max_r * row_bytes), mhcudaMemoryAllocationFailure);
+      MHB_CHECK(gen, sl.w.ensure(max_n * 4 + 16), mhcudaMemoryAllocationFailure);
+      MHB_CHECK(gen, sl.c.ensure(max_n * 4 + 16), mhcudaMemoryAllocationFailure);
+      MHB_CHECK(gen, sl.ip.ensure((max_r + 1) * 4), mhcudaMemoryAllocationFailure);
+      MHB_CHECK(gen, sl.out.ensure(max_r * row_bytes), mhcudaMemoryAllocationFailure);
+    }
+    HashPlan big{};
+    big.nchunks = max_chunks;
+    HashArgs unused{};
+    const MHCUDAResult pr = prepare_launch(gen, 0, 0, big, &unused);
+    if (pr != mhcudaSuccess) return pr;
+  }
+
+  MHCUDAResult r = mhcudaSuccess;
+  for (uint32_t g = 0; g < groups.size() && r == mhcudaSuccess; ++g) {
+    const uint32_t m0 = groups[g].m0, m1 = groups[g].m1;
+    const uint64_t gn = groups[g].nnz, gr = groups[g].rows;
+    const uint32_t k = g % Gen::kBatchSlots;
     Gen::Slot &sl = gen->slots[k];
     r = retire(k);
     if (r != mhcudaSuccess) break;
-    if (gr == 0) {  // only empty matrices
-      m0 = m1;
-      continue;
-    }
+    if (gr == 0) continue;  // only empty matrices
     const uint32_t R = static_cast<uint32_t>(gr), N = static_cast<uint32_t>(gn);
     MHB_CHECK(gen, sl.hw.ensure(static_cast<size_t>(N) * 4), mhcudaMemoryAllocationFailure);
     MHB_CHECK(gen, sl.hc.ensure(static_cast<size_t>(N) * 4), mhcudaMemoryAllocationFailure);
@@ -1302,9 +1366,8 @@ enum MHCUDAResult mhcuda_calc_batch(const MinhashCudaGenerator *gen, uint32_t co
     sl.pending_out = nullptr;
     pending[k] = Pending{m0, m1};
     MHB_DEBUG(gen, "batch group %u: matrices [%u, %u) rows %u nnz %u\n", g, m0, m1, R, N);
-    m0 = m1;
   }
-  for (uint32_t k = 0; k < 2; ++k) {
+  for (uint32_t k = 0; k < Gen::kBatchSlots; ++k) {
     const MHCUDAResult rr = retire(k);
     if (r == mhcudaSuccess) r = rr;
   }

@@ -253,10 +253,15 @@ def test_near_integer_quotients():
     check(sp.vstack([single, mixed]).tocsr(), samples, params)
 
 
-@pytest.mark.parametrize("group_nnz", [1500, 20000])
-def test_batch_groups_and_empty_matrices(monkeypatch, group_nnz):
-    """mhcuda_calc_batch cut into several pipelined groups (including empty
-    matrices and matrices larger than a group) equals one calc per matrix."""
+@pytest.mark.parametrize("knob,group_nnz", [("MHCUDA_B200_BLOCK_NNZ", 1500),
+                                            ("MHCUDA_B200_BLOCK_NNZ", 20000),
+                                            ("MHCUDA_B200_BATCH_GROUP_NNZ", 20000),
+                                            ("MHCUDA_B200_BATCH_GROUP_NNZ", 3000)])
+def test_batch_groups_and_empty_matrices(monkeypatch, knob, group_nnz):
+    """mhcuda_calc_batch cut into several pipelined groups -- constant ones
+    (MHCUDA_B200_BLOCK_NNZ) or growing from an eighth of the cap with a small
+    last group (MHCUDA_B200_BATCH_GROUP_NNZ) -- including empty matrices and
+    matrices larger than a group, equals one calc per matrix."""
     import ctypes
     rng = np.random.default_rng(group_nnz)
     dim, samples = 3000, 64
@@ -269,7 +274,7 @@ def test_batch_groups_and_empty_matrices(monkeypatch, group_nnz):
     co = O.COracle(*params)
     with engine_gen(dim, samples, deferred=True) as eng:
         eng.assign(*params)
-        monkeypatch.setenv("MHCUDA_B200_BLOCK_NNZ", str(group_nnz))
+        monkeypatch.setenv(knob, str(group_nnz))
         arrs = [(m.data.astype(np.float32), m.indices.astype(np.uint32),
                  m.indptr.astype(np.uint32)) for m in mats]
         outs = [np.full((m.shape[0], samples, 2), 3, np.uint32) for m in mats]
