@@ -236,7 +236,10 @@ uint64_t tune_key(uint64_t nnz, uint64_t rows) {
   return (lg(nnz + 1) << 8) | lg(avg + 1);
 }
 
-HashPlan make_plan(const Gen *gen, uint64_t nnz, uint64_t rows, const TuneChoice *force = nullptr) {
+// min_items: items per resident warp the chunk is capped to give (8 for the
+// engine's own calls; the server asks for 2, its launches overlap).
+HashPlan make_plan(const Gen *gen, uint64_t nnz, uint64_t rows, const TuneChoice *force = nullptr,
+                   uint32_t min_items = 8) {
   HashPlan p{};
   const uint32_t s_pad = gen->s_pad;
   TuneChoice tuned{};
@@ -287,12 +290,12 @@ HashPlan make_plan(const Gen *gen, uint64_t nnz, uint64_t rows, const TuneChoice
   const uint64_t avg_row = rows ? (nnz + rows - 1) / rows : 1;
   chunk = std::max<uint64_t>(chunk, std::min<uint64_t>(4 * avg_row, 1024));
   // Warps take items round-robin (static), so a launch with few items per
-  // warp ends on a ragged last wave: keep at least 8 items per resident warp
-  // even if rows then span chunks (their partials are merged by finalize).
+  // warp ends on a ragged last wave: keep at least min_items items per
+  // resident warp even if rows then span chunks (their partials are merged
+  // by finalize).
   {
-    const uint64_t min_items = resident_warps * 8;
-    chunk = std::min<uint64_t>(
-        chunk, std::max<uint64_t>(64, (nnz * p.ntiles + min_items - 1) / min_items));
+    const uint64_t want = resident_warps * std::max<uint32_t>(1, min_items);
+    chunk = std::min<uint64_t>(chunk, std::max<uint64_t>(64, (nnz * p.ntiles + want - 1) / want));
   }
   const int forced = env_int("MHCUDA_B200_CHUNK", 0);
   if (forced > 0) chunk = static_cast<uint64_t>(forced);
@@ -770,8 +773,9 @@ MHCUDAResult init_params(Gen *gen, uint32_t seed) {
 
 namespace mhb {
 
-HashPlan plan_for_generator(const MinhashCudaGenerator_ *gen, uint64_t nnz, uint64_t rows) {
-  return make_plan(gen, nnz, rows);
+HashPlan plan_for_generator(const MinhashCudaGenerator_ *gen, uint64_t nnz, uint64_t rows,
+                            uint32_t min_items) {
+  return make_plan(gen, nnz, rows, nullptr, min_items);
 }
 
 bool generator_view(const MinhashCudaGenerator_ *gen, GeneratorView *view) {

@@ -536,37 +536,64 @@ __global__ void __launch_bounds__(kHashBlock, MINB) hash_kernel(const HashArgs a
   }
 }
 
-// Merge the partials of every row that leaves its own chunk.
+// Merge the partials of every row that leaves its own chunk: one warp per
+// (chunk owning such a row, tile of 32 samples), lanes over samples.  The
+// chunks the row runs through are read in position order with unconditional
+// loads, kFinalizeUnroll in flight (a row of 50,000 nnz cut into 64-nnz
+// chunks has ~780 partials), and a strict '<' keeps the earliest position on
+// ties, as the scan of kernel.cu:106 does.
+constexpr uint32_t kFinalizeUnroll = 8;
+
 __global__ void finalize_kernel(const HashArgs a) {
   if (*a.status & kStatusBadIndptr) return;
   const uint32_t lane = threadIdx.x & 31u;
-  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  const uint64_t gw = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) >> 5;
+  const uint64_t nw = (gridDim.x * static_cast<uint64_t>(blockDim.x)) >> 5;
   const uint32_t base = a.indptr[0];
-  for (uint32_t c = gw; c < a.nchunks; c += nw) {
+  const uint32_t stiles = (a.samples + 31) / 32;
+  const uint64_t items = static_cast<uint64_t>(a.nchunks) * stiles;
+  const size_t stride = 2 * static_cast<size_t>(a.s_pad);  // one chunk's two slots
+  for (uint64_t it = gw; it < items; it += nw) {
+    const uint32_t c = static_cast<uint32_t>(it / stiles);
+    const uint32_t s = static_cast<uint32_t>(it - static_cast<uint64_t>(c) * stiles) * 32 + lane;
     const uint32_t r0 = a.chunk_row[c];
     const uint32_t r1 = (c + 1 < a.nchunks) ? a.chunk_row[c + 1] : a.rows;
     if (r1 <= r0) continue;
     const uint32_t row = r1 - 1;
     const uint32_t end = a.indptr[row + 1] - base;
     const uint32_t ce = c * a.chunk + min(a.chunk, a.nnz - c * a.chunk);
-    if (end <= ce) continue;
+    if (end <= ce || s >= a.samples) continue;
     const uint32_t c_last = (end - 1) / a.chunk;
-    uint32_t *o = a.out + static_cast<size_t>(row) * a.samples * 2;
-    for (uint32_t s = lane; s < a.samples; s += 32) {
-      size_t off = static_cast<size_t>(2 * c + 1) * a.s_pad + s;
-      float mn = a.part_ln[off];
-      uint2 kt = a.part_kt[off];
-      for (uint32_t cc = c + 1; cc <= c_last; ++cc) {
-        off = static_cast<size_t>(2 * cc) * a.s_pad + s;
-        const float m2 = a.part_ln[off];
-        if (m2 < mn) {
-          mn = m2;
-          kt = a.part_kt[off];
-        }
+    size_t off = static_cast<size_t>(2 * c + 1) * a.s_pad + s;
+    float mn = a.part_ln[off];
+    uint2 kt = a.part_kt[off];
+    off = static_cast<size_t>(2 * (c + 1)) * a.s_pad + s;
+    uint32_t cc = c + 1;
+    for (; cc + kFinalizeUnroll - 1 <= c_last; cc += kFinalizeUnroll) {
+      float m[kFinalizeUnroll];
+      uint2 k[kFinalizeUnroll];
+#pragma unroll
+      for (uint32_t u = 0; u < kFinalizeUnroll; ++u) {
+        m[u] = a.part_ln[off + u * stride];
+        k[u] = a.part_kt[off + u * stride];
       }
-      *reinterpret_cast<uint2 *>(o + 2 * s) = final_pair(kt.x, __uint_as_float(kt.y));
+#pragma unroll
+      for (uint32_t u = 0; u < kFinalizeUnroll; ++u) {
+        const bool lt = m[u] < mn;
+        mn = lt ? m[u] : mn;
+        kt = lt ? k[u] : kt;
+      }
+      off += kFinalizeUnroll * stride;
     }
+    for (; cc <= c_last; ++cc, off += stride) {
+      const float m2 = a.part_ln[off];
+      const uint2 k2 = a.part_kt[off];
+      const bool lt = m2 < mn;
+      mn = lt ? m2 : mn;
+      kt = lt ? k2 : kt;
+    }
+    uint32_t *o = a.out + (static_cast<size_t>(row) * a.samples + s) * 2;
+    *reinterpret_cast<uint2 *>(o) = final_pair(kt.x, __uint_as_float(kt.y));
   }
 }
 
@@ -610,10 +637,11 @@ cudaError_t launch_hash(const HashArgs &a, const HashPlan &plan, cudaStream_t st
 }
 
 cudaError_t launch_finalize(const HashArgs &a, cudaStream_t stream) {
-  const uint32_t warps_per_block = 8;
-  uint32_t blocks = (a.nchunks + warps_per_block - 1) / warps_per_block;
-  if (blocks > 4096) blocks = 4096;
-  finalize_kernel<<<blocks, 32 * warps_per_block, 0, stream>>>(a);
+  const uint64_t warps_per_block = 8;
+  const uint64_t items = static_cast<uint64_t>(a.nchunks) * ((a.samples + 31) / 32);
+  uint64_t blocks = (items + warps_per_block - 1) / warps_per_block;
+  if (blocks > 8192) blocks = 8192;
+  finalize_kernel<<<static_cast<unsigned>(blocks), 32 * warps_per_block, 0, stream>>>(a);
   return cudaGetLastError();
 }
 

@@ -119,6 +119,7 @@ struct MinhashCudaServer_ {
   uint64_t max_unit_evals = 128ull << 20;   // nnz*samples: high-priority batch limit
   uint64_t max_batch_evals = 512ull << 20;  // nnz*samples of one lane batch
   uint32_t max_low_inflight = 6;            // low-priority batches out at once (lanes - 2)
+  uint64_t zero_copy_max_bytes = ~0ull;     // CSR bytes of a batch read from mapped memory
   uint32_t low_inflight = 0;
   std::vector<Lane> lanes;
 
@@ -255,7 +256,7 @@ MHCUDAResult MinhashCudaServer_::run_units(Lane &lane, const std::vector<Unit> &
   // High-priority batches of a lane with mapped staging use no copy engine:
   // the kernels read the CSR from the staging and write the hashes into
   // mapped host memory, so they never queue behind large batches' copies.
-  const bool zc = high && lane.zero_copy;
+  const bool zc = high && lane.zero_copy && N * 8 + R * 4 <= zero_copy_max_bytes;
   for (size_t k = 0; k < units.size(); ++k) {
     const Unit &u = units[k];
     const uint32_t b = u.req->rows[u.r0];
@@ -278,20 +279,11 @@ MHCUDAResult MinhashCudaServer_::run_units(Lane &lane, const std::vector<Unit> &
   if (!zc) flush_run();
   lane.hip[R] = static_cast<uint32_t>(N);
   const uint32_t s_pad = g.s_pad;
-  mhb::HashPlan plan = mhb::plan_for_generator(units.front().req->gen, N, R);
+  // Batches are small next to a plain call: at least two waves of warp items
+  // even when rows are long (the plain plan keeps a few rows per chunk);
+  // several lanes' launches overlap, so two are enough.
+  mhb::HashPlan plan = mhb::plan_for_generator(units.front().req->gen, N, R, 2);
   const int bps = mhb::hash_blocks_per_sm(plan.spl, plan.minb);
-  // Batches are small next to a plain call: cut at least two waves of warp
-  // items even when rows are long (the plain plan keeps a few rows per chunk).
-  {
-    const uint64_t resident_warps =
-        static_cast<uint64_t>(sm_count) * bps * (mhb::kHashBlock / 32);
-    uint64_t chunk = (N * plan.ntiles + 2 * resident_warps - 1) / (2 * resident_warps);
-    chunk = std::max<uint64_t>(64, (chunk + 31) & ~31ull);
-    if (chunk < plan.chunk) {
-      plan.chunk = static_cast<uint32_t>(chunk);
-      plan.nchunks = static_cast<uint32_t>(N == 0 ? 1 : (N + chunk - 1) / chunk);
-    }
-  }
   // Keep the chunk table and partials inside the lane's fixed scratch:
   // nchunks*4 <= unit, 2*nchunks*s_pad*4 <= 4*unit, 2*nchunks*s_pad*8 <= 8*unit.
   const uint64_t max_chunks = std::max<uint64_t>(
@@ -546,6 +538,7 @@ MinhashCudaServer *mhcuda_server_start(uint32_t devices, uint64_t hbm_budget_byt
   srv->verbosity = verbosity;
   srv->max_unit_evals = env_u64("MHCUDA_B200_SERVER_UNIT_EVALS", srv->max_unit_evals);
   srv->max_batch_evals = env_u64("MHCUDA_B200_SERVER_BATCH_EVALS", srv->max_batch_evals);
+  srv->zero_copy_max_bytes = env_u64("MHCUDA_B200_SERVER_ZERO_COPY_MAX_BYTES", ~0ull);
   srv->max_low_inflight = static_cast<uint32_t>(std::min<uint64_t>(
       lanes, env_u64("MHCUDA_B200_SERVER_LOW_INFLIGHT", lanes > 2 ? lanes - 2 : 1)));
   cudaDeviceGetAttribute(&srv->sm_count, cudaDevAttrMultiProcessorCount, dev);

@@ -103,7 +103,9 @@ struct GeneratorView {
   cudaStream_t stream;
 };
 bool generator_view(const MinhashCudaGenerator_ *gen, GeneratorView *view);
-// The engine's work decomposition for `nnz` entries in `rows` rows.
-HashPlan plan_for_generator(const MinhashCudaGenerator_ *gen, uint64_t nnz, uint64_t rows);
+// The engine's work decomposition for `nnz` entries in `rows` rows, with at
+// least `min_items` warp items per resident warp where chunks allow.
+HashPlan plan_for_generator(const MinhashCudaGenerator_ *gen, uint64_t nnz, uint64_t rows,
+                            uint32_t min_items = 8);
 
 }  // namespace mhb

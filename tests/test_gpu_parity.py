@@ -233,6 +233,24 @@ def test_row_block_pipeline_reports_bad_column_in_late_block(monkeypatch):
         assert out.shape == (400, 64, 2)
 
 
+@pytest.mark.parametrize("chunk,samples", [(64, 128), (96, 200), (64, 31)])
+def test_rows_spanning_hundreds_of_chunks(monkeypatch, chunk, samples):
+    """Rows of up to 50,000 nnz cut into 64/96-nnz chunks: every such row is
+    merged from hundreds of partials by finalize (position order, earliest
+    position on ties), and sample counts that are not a multiple of 32 leave
+    a ragged last tile."""
+    rng = np.random.default_rng(chunk + samples)
+    dim = 60000
+    m = random_csr(rng, 40, dim, 30, long_rows=[(0, 50000), (3, 20000), (4, 777), (39, 31000)])
+    params = gamma_params(rng, dim, samples)
+    monkeypatch.setenv("MHCUDA_B200_CHUNK", str(chunk))
+    with engine_gen(dim, samples, deferred=True) as eng:
+        eng.assign(*params)
+        got = eng.calc_csr(m)
+    want = O.COracle(*params).hash_csr(m, lnw=device_logf(m.data))
+    np.testing.assert_array_equal(got, want)
+
+
 def test_near_integer_quotients():
     """w/r + beta within 1e-9..1e-3 of an integer on either side: the fast
     reciprocal path must hand every such case to the exact IEEE quotient."""
