@@ -80,21 +80,30 @@ __device__ __forceinline__ bool fast_t(float w, float r, float b, float &t) {
   return fabsf(__fsub_rn(f, 0.5f)) < __fsub_rn(0.5f, m);  // NaN -> false
 }
 
-// One (nnz, sample) evaluation, kernel.cu:101-109, given t.
-__device__ __forceinline__ void wmh_update(float t, float r, float c, float b, uint32_t d,
-                                           float &mn, uint32_t &kk, float &tf) {
+// One (nnz, sample) evaluation, kernel.cu:101-109, given t: keeps the
+// minimum and the position `p` it came from.
+__device__ __forceinline__ void wmh_update(float t, float r, float c, float b, uint32_t p,
+                                           float &mn, uint32_t &pos) {
   const float tb = __fsub_rn(t, b);
   const float ln_a = __fsub_rn(__fmaf_rn(-tb, r, c), r);
   const bool lt = ln_a < mn;
   mn = lt ? ln_a : mn;
-  kk = lt ? d : kk;
-  tf = lt ? t : tf;
+  pos = lt ? p : pos;
 }
 
-__device__ __forceinline__ uint2 final_pair(uint32_t k, float t) {
-  // (uint32)(int32)t as kernel.cu:108; the GPU conversion saturates.
-  return k == kNone ? make_uint2(kNone, kNone)
-                    : make_uint2(k, static_cast<uint32_t>(static_cast<int32_t>(t)));
+// The output pair of kernel.cu:108 for sample s whose minimum came from the
+// entry at relative position `pos`: k = cols[pos] and t recomputed from the
+// entry with the exact quotient.  Every evaluation used that same t (fast_t
+// only decides t when it equals the exact one), so tracking the position
+// instead of (k, t) changes nothing but the work per evaluation.
+// (uint32)(int32)t as kernel.cu:108; the GPU conversion saturates.
+__device__ __forceinline__ uint2 resolve(const HashArgs &a, uint32_t pos, uint32_t s) {
+  if (pos == kNone) return make_uint2(kNone, kNone);
+  const uint32_t k = a.cols[pos];
+  const float w = logf(a.weights[pos]);
+  const float *col = a.params + static_cast<size_t>(k) * 3 * a.s_pad + s;
+  const float t = exact_t(w, col[0], col[2 * static_cast<size_t>(a.s_pad)]);
+  return make_uint2(k, static_cast<uint32_t>(static_cast<int32_t>(t)));
 }
 
 // chunk_row[c] = first row whose first position is >= c*chunk (rows if none).
@@ -126,14 +135,12 @@ __global__ void plan_kernel(const HashArgs a) {
 template <int SPL>
 struct RowState {
   float mn[SPL];
-  uint32_t kk[SPL];
-  float tf[SPL];
+  uint32_t pos[SPL];  // relative position of the minimum, kNone if none
   __device__ __forceinline__ void reset() {
 #pragma unroll
     for (int j = 0; j < SPL; ++j) {
       mn[j] = FLT_MAX;
-      kk[j] = kNone;
-      tf[j] = 0.0f;
+      pos[j] = kNone;
     }
   }
 };
@@ -144,7 +151,7 @@ __device__ __forceinline__ void store_final(const HashArgs &a, uint32_t row, uin
   uint32_t *o = a.out + (static_cast<size_t>(row) * a.samples + s0) * 2;
 #pragma unroll
   for (int j = 0; j < SPL; ++j) {
-    if (s0 + j < a.samples) *reinterpret_cast<uint2 *>(o + 2 * j) = final_pair(st.kk[j], st.tf[j]);
+    if (s0 + j < a.samples) *reinterpret_cast<uint2 *>(o + 2 * j) = resolve(a, st.pos[j], s0 + j);
   }
 }
 
@@ -155,7 +162,7 @@ __device__ __forceinline__ void store_partial(const HashArgs &a, uint32_t slot, 
 #pragma unroll
   for (int j = 0; j < SPL; ++j) {
     a.part_ln[off + j] = st.mn[j];
-    a.part_kt[off + j] = make_uint2(st.kk[j], __float_as_uint(st.tf[j]));
+    a.part_kt[off + j] = make_uint2(st.pos[j], 0u);
   }
 }
 
@@ -310,23 +317,20 @@ __device__ __forceinline__ F2 fma2(F2 a, F2 b, F2 c) {
   return r;
 }
 
-// Selects for samples j and j+1 given their ln_a pair.
+// Selects for samples j and j+1 given their ln_a pair (position p).
 template <int SPL>
-__device__ __forceinline__ void update_pair(F2 ln_a, float t0, float t1, uint32_t d, int j,
-                                            RowState<SPL> &st) {
+__device__ __forceinline__ void update_pair(F2 ln_a, uint32_t p, int j, RowState<SPL> &st) {
   float l0, l1;
   split(ln_a, l0, l1);
   const bool lt0 = l0 < st.mn[j], lt1 = l1 < st.mn[j + 1];
   st.mn[j] = lt0 ? l0 : st.mn[j];
-  st.kk[j] = lt0 ? d : st.kk[j];
-  st.tf[j] = lt0 ? t0 : st.tf[j];
+  st.pos[j] = lt0 ? p : st.pos[j];
   st.mn[j + 1] = lt1 ? l1 : st.mn[j + 1];
-  st.kk[j + 1] = lt1 ? d : st.kk[j + 1];
-  st.tf[j + 1] = lt1 ? t1 : st.tf[j + 1];
+  st.pos[j + 1] = lt1 ? p : st.pos[j + 1];
 }
 
 template <int SPL>
-__device__ __forceinline__ void eval_all(const Params<SPL> &p, float w, uint32_t d, bool active,
+__device__ __forceinline__ void eval_all(const Params<SPL> &p, float w, uint32_t pos, bool active,
                                          RowState<SPL> &st) {
   float t[SPL];
   bool undecided = false;
@@ -375,12 +379,12 @@ __device__ __forceinline__ void eval_all(const Params<SPL> &p, float w, uint32_t
       const F2 rr = f2(p.r.v[j], p.r.v[j + 1]);
       const F2 nb = sub2(f2(p.b.v[j], p.b.v[j + 1]), f2(t[j], t[j + 1]));
       const F2 ln_a = sub2(fma2(nb, rr, f2(p.c.v[j], p.c.v[j + 1])), rr);
-      update_pair<SPL>(ln_a, t[j], t[j + 1], d, j, st);
+      update_pair<SPL>(ln_a, pos, j, st);
     }
   } else {
 #pragma unroll
     for (int j = 0; j < SPL; ++j)
-      wmh_update(t[j], p.r.v[j], p.c.v[j], p.b.v[j], d, st.mn[j], st.kk[j], st.tf[j]);
+      wmh_update(t[j], p.r.v[j], p.c.v[j], p.b.v[j], pos, st.mn[j], st.pos[j]);
   }
 }
 
@@ -496,13 +500,13 @@ __global__ void __launch_bounds__(kHashBlock, MINB) hash_kernel(const HashArgs a
         while (i + 1 < seg) {
           dB = cl[i + 1];
           if (active && dB < a.dim) B.load(pbase + dB * col_stride, a.s_pad);
-          if (dA < a.dim) eval_all<SPL>(A, lw[i], dA, active, st);
+          if (dA < a.dim) eval_all<SPL>(A, lw[i], ws + i, active, st);
           else if (lane == 0) atomicOr(a.status, kStatusBadColumn);
           if (i + 2 < n) {
             dA = cl[i + 2];
             if (active && dA < a.dim) A.load(pbase + dA * col_stride, a.s_pad);
           }
-          if (dB < a.dim) eval_all<SPL>(B, lw[i + 1], dB, active, st);
+          if (dB < a.dim) eval_all<SPL>(B, lw[i + 1], ws + i + 1, active, st);
           else if (lane == 0) atomicOr(a.status, kStatusBadColumn);
           i += 2;
         }
@@ -511,7 +515,7 @@ __global__ void __launch_bounds__(kHashBlock, MINB) hash_kernel(const HashArgs a
             dB = cl[i + 1];
             if (active && dB < a.dim) B.load(pbase + dB * col_stride, a.s_pad);
           }
-          if (dA < a.dim) eval_all<SPL>(A, lw[i], dA, active, st);
+          if (dA < a.dim) eval_all<SPL>(A, lw[i], ws + i, active, st);
           else if (lane == 0) atomicOr(a.status, kStatusBadColumn);
           ++i;
           A = B;
@@ -566,34 +570,34 @@ __global__ void finalize_kernel(const HashArgs a) {
     const uint32_t c_last = (end - 1) / a.chunk;
     size_t off = static_cast<size_t>(2 * c + 1) * a.s_pad + s;
     float mn = a.part_ln[off];
-    uint2 kt = a.part_kt[off];
+    uint32_t kp = a.part_kt[off].x;
     off = static_cast<size_t>(2 * (c + 1)) * a.s_pad + s;
     uint32_t cc = c + 1;
     for (; cc + kFinalizeUnroll - 1 <= c_last; cc += kFinalizeUnroll) {
       float m[kFinalizeUnroll];
-      uint2 k[kFinalizeUnroll];
+      uint32_t k[kFinalizeUnroll];
 #pragma unroll
       for (uint32_t u = 0; u < kFinalizeUnroll; ++u) {
         m[u] = a.part_ln[off + u * stride];
-        k[u] = a.part_kt[off + u * stride];
+        k[u] = a.part_kt[off + u * stride].x;
       }
 #pragma unroll
       for (uint32_t u = 0; u < kFinalizeUnroll; ++u) {
         const bool lt = m[u] < mn;
         mn = lt ? m[u] : mn;
-        kt = lt ? k[u] : kt;
+        kp = lt ? k[u] : kp;
       }
       off += kFinalizeUnroll * stride;
     }
     for (; cc <= c_last; ++cc, off += stride) {
       const float m2 = a.part_ln[off];
-      const uint2 k2 = a.part_kt[off];
+      const uint32_t k2 = a.part_kt[off].x;
       const bool lt = m2 < mn;
       mn = lt ? m2 : mn;
-      kt = lt ? k2 : kt;
+      kp = lt ? k2 : kp;
     }
     uint32_t *o = a.out + (static_cast<size_t>(row) * a.samples + s) * 2;
-    *reinterpret_cast<uint2 *>(o) = final_pair(kt.x, __uint_as_float(kt.y));
+    *reinterpret_cast<uint2 *>(o) = resolve(a, kp, s);
   }
 }
 

@@ -63,7 +63,7 @@ struct HashArgs {
   uint32_t ntiles;
   uint32_t *chunk_row;       // [nchunks] first row owned by each chunk
   float *part_ln;            // [2*nchunks][s_pad] partial minima
-  uint2 *part_kt;            // [2*nchunks][s_pad] partial (k, float bits of t)
+  uint2 *part_kt;            // [2*nchunks][s_pad] partial (position of the minimum, 0)
   uint32_t *out;             // [rows][samples][2]
   uint32_t *status;          // device status word
   uint32_t host_csr;         // weights/cols/indptr/out are mapped host memory
