@@ -40,7 +40,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-ccbin",
               "-I" + INCLUDE, "--expt-relaxed-constexpr"]
 
 ENGINE_SOURCES = ["hash_kernels.cu", "param_kernels.cu", "engine.cu", "noalloc.cu", "server.cu",
-                  "lsh.cu"]
+                  "lsh.cu", "host_copy.cc"]
 HEADERS = ["wmh_internal.h"]
 
 EXT_SUFFIX = sysconfig.get_config_var("EXT_SUFFIX") or ".so"

@@ -32,6 +32,7 @@
 
 using mhb::HashArgs;
 using mhb::HashPlan;
+using mhb::stream_copy;
 
 namespace {
 
@@ -399,7 +400,7 @@ void par_memcpy(void *dst, const void *src, size_t bytes) {
   const size_t kSplit = static_cast<size_t>(8) << 20;
   const unsigned n = bytes < kSplit ? 1u : host_threads();
   if (n == 1) {
-    memcpy(dst, src, bytes);
+    stream_copy(dst, src, bytes);
     return;
   }
   const size_t part = (((bytes + n - 1) / n) + 4095) & ~static_cast<size_t>(4095);
@@ -409,7 +410,7 @@ void par_memcpy(void *dst, const void *src, size_t bytes) {
     if (off >= bytes) break;
     const size_t len = std::min(part, bytes - off);
     pool.emplace_back([=]() {
-      memcpy(static_cast<char *>(dst) + off, static_cast<const char *>(src) + off, len);
+      stream_copy(static_cast<char *>(dst) + off, static_cast<const char *>(src) + off, len);
     });
   }
   for (auto &th : pool) th.join();
@@ -477,28 +478,14 @@ void stage_entries(const HostCsr &in, uint64_t b0, size_t n, float *w, uint32_t 
   constexpr size_t kSplit = size_t{2} << 20;
   if (in.w64) {
     const double *src = static_cast<const double *>(in.weights) + b0;
-    par_for(n, kSplit, [=](size_t b, size_t e) {
-      for (size_t i = b; i < e; ++i) w[i] = static_cast<float>(src[i]);
-    });
+    par_for(n, kSplit, [=](size_t b, size_t e) { mhb::convert_f64_to_f32(w + b, src + b, e - b); });
   } else {
     par_memcpy(w, static_cast<const float *>(in.weights) + b0, n * sizeof(float));
   }
-  if (in.cols64 == 1) {
-    const int64_t *src = static_cast<const int64_t *>(in.cols) + b0;
-    par_for(n, kSplit, [=](size_t b, size_t e) {
-      for (size_t i = b; i < e; ++i) {
-        const int64_t v = src[i];
-        c[i] = (v < 0 || v > 0xFFFFFFFFll) ? 0xFFFFFFFFu : static_cast<uint32_t>(v);
-      }
-    });
-  } else if (in.cols64 == 2) {
+  if (in.cols64) {
+    // int64 and uint64 alike: a negative int64 has its high bits set.
     const uint64_t *src = static_cast<const uint64_t *>(in.cols) + b0;
-    par_for(n, kSplit, [=](size_t b, size_t e) {
-      for (size_t i = b; i < e; ++i) {
-        const uint64_t v = src[i];
-        c[i] = v > 0xFFFFFFFFull ? 0xFFFFFFFFu : static_cast<uint32_t>(v);
-      }
-    });
+    par_for(n, kSplit, [=](size_t b, size_t e) { mhb::convert_i64_to_u32(c + b, src + b, e - b); });
   } else {
     par_memcpy(c, static_cast<const uint32_t *>(in.cols) + b0, n * sizeof(uint32_t));
   }
@@ -1211,7 +1198,7 @@ enum MHCUDAResult mhcuda_calc_batch(const MinhashCudaGenerator *gen, uint32_t co
     for (unsigned t = 0; t < nth; ++t) {
       pool.emplace_back([&, t]() {
         for (uint32_t i = pd.first + t; i < pd.last; i += nth)
-          if (lengths[i]) memcpy(outputs[i], src + off[i - pd.first], lengths[i] * row_bytes);
+          if (lengths[i]) stream_copy(outputs[i], src + off[i - pd.first], lengths[i] * row_bytes);
       });
     }
     for (auto &th : pool) th.join();
@@ -1327,8 +1314,8 @@ enum MHCUDAResult mhcuda_calc_batch(const MinhashCudaGenerator *gen, uint32_t co
             if (!len) continue;
             const uint32_t b = rows[i][0];
             const uint64_t po = moff[i - m0], ro = roff[i - m0];
-            memcpy(sw + po, weights[i] + b, nnz_of[i] * 4);
-            memcpy(sc + po, cols[i] + b, nnz_of[i] * 4);
+            stream_copy(sw + po, weights[i] + b, nnz_of[i] * 4);
+            stream_copy(sc + po, cols[i] + b, nnz_of[i] * 4);
             for (uint64_t x = 0; x < len; ++x)
               si[ro + x] = static_cast<uint32_t>(po + (rows[i][x] - b));
           }

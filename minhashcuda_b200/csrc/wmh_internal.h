@@ -90,6 +90,14 @@ cudaError_t launch_unpack_params(const float *params, uint32_t which, uint32_t d
                                  cudaStream_t stream);
 cudaError_t launch_logf(const float *in, float *out, size_t n, cudaStream_t stream);
 
+// memcpy for host staging moves: non-temporal stores for large pieces
+// (host_copy.cc).
+void stream_copy(void *dst, const void *src, size_t bytes);
+// float64 -> float32 (round to nearest) and 64-bit -> uint32 (values outside
+// [0, 2^32) become 0xFFFFFFFF), with non-temporal stores for large pieces.
+void convert_f64_to_f32(float *dst, const double *src, size_t n);
+void convert_i64_to_u32(uint32_t *dst, const uint64_t *src, size_t n);
+
 // Read-only view of a generator's fields for entry points that live outside
 // engine.cu (engine.cu).
 struct GeneratorView {
