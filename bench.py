@@ -751,8 +751,12 @@ def main():
     gen = lib.mhcuda_init(w.dim, w.samples, w.seed, 0, dev_mask, 0, ctypes.byref(status))
     assert gen, f"mhcuda_init failed: {status.value}"
     stream = torch.cuda.Stream()
+    # Each rank hashes its own shard: rows [rank*R, (rank+1)*R) of the seeded
+    # workload (every draw is keyed by absolute row index), so N ranks hash N
+    # distinct blocks of R rows (weak scaling, no data-path collective).
+    row0 = rank * w.rows
     with torch.cuda.stream(stream):
-        indptr, cols, weights, nnz = synth.device_csr(w, 0, w.rows, stream=stream)
+        indptr, cols, weights, nnz = synth.device_csr(w, row0, w.rows, stream=stream)
     torch.cuda.synchronize()
     log(f"[rank {rank}] workload {w.name}: rows={w.rows} nnz={nnz} "
         f"generated in {time.perf_counter() - t0:.1f}s")
@@ -808,7 +812,9 @@ def main():
     barrier()
     ms_step = max_over_ranks(ms_total / args.steps)
     evals = nnz * S
-    value = evals * world / (ms_step / 1e3)
+    from minhashcuda_b200.replicas import sum_over_ranks
+    job_evals = sum_over_ranks(evals, pg, device="cuda")
+    value = job_evals / (ms_step / 1e3)
 
     hash_ms_launch = hash_ms.value / max(1, launches.value)
     alg_bytes = 12 * nnz * S + 8 * nnz + 4 * (R + 1) + 8 * R * S
@@ -879,7 +885,7 @@ def main():
         wall = (time.perf_counter() - t0) / args.steps
         e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
         same = bool(torch.equal(h_o.cuda(), out))
-        e2e = {"value": evals * world / (e2e_ms / 1e3), "unit": UNIT,
+        e2e = {"value": job_evals / (e2e_ms / 1e3), "unit": UNIT,
                "h2d_bytes_per_step": 8 * nnz + 4 * (R + 1), "d2h_bytes_per_step": 8 * R * S,
                "ms_per_step": e2e_ms, "wall_ms_per_step": wall * 1e3,
                "matches_device_path": same}

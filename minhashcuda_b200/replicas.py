@@ -42,3 +42,15 @@ def max_over_ranks(value: float, dist=None, device=None) -> float:
     t = torch.tensor([float(value)], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def sum_over_ranks(value: float, dist=None, device=None) -> float:
+    """The sum of `value` over all ranks (the job's work is every rank's
+    shard); `value` itself when there is no process group."""
+    if dist is None or not dist.is_initialized():
+        return value
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+

@@ -24,7 +24,7 @@ def _rank_main(rank, world, port, result_dir):
         sys.path.insert(0, p)
     import torch.distributed as dist
     import oracle as O
-    from minhashcuda_b200.replicas import max_over_ranks, shard_rows
+    from minhashcuda_b200.replicas import max_over_ranks, shard_rows, sum_over_ranks
     from wmh_testlib import gamma_params, random_csr
     dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
                             world_size=world)
@@ -37,6 +37,7 @@ def _rank_main(rank, world, port, result_dir):
     parts = [None] * world
     dist.all_gather_object(parts, (r0, r1, part))
     slowest = max_over_ranks(float(rank + 1), dist)
+    total = sum_over_ranks(float(r1 - r0), dist)
     dist.barrier()
     if rank == 0:
         whole = O.COracle(*params).hash_csr(m)
@@ -46,6 +47,7 @@ def _rank_main(rank, world, port, result_dir):
             assert a[1] == b[0]
         np.testing.assert_array_equal(np.concatenate([p[2] for p in parts]), whole)
         assert slowest == float(world)
+        assert total == float(m.shape[0])
         open(os.path.join(result_dir, "ok"), "w").write("ok")
     dist.destroy_process_group()
 
