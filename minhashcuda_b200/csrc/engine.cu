@@ -529,7 +529,8 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
   // first block is small -- 16M nnz, still a few waves of warp items -- and
   // later ones grow geometrically to block_nnz; the factor keeps each block's
   // copy-in (8 B per nnz) shorter than the previous block's hashing (samples
-  // evals per nnz): about samples / 112 on a B200 with a Gen5 x16 link.
+  // evals per nnz), with slack: max(1.08, samples / 120) on a B200 with a
+  // Gen5 x16 link.
   // MHCUDA_B200_BLOCK_NNZ gives constant blocks.
   struct Block {
     uint32_t r0, r1;
@@ -539,7 +540,7 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
     uint64_t cur = forced > 0 ? block_nnz
                               : std::min(block_nnz, std::max<uint64_t>(block_nnz / 32, 16ull << 20));
     const double growth =
-        forced > 0 ? 1.0 : std::min(2.0, std::max(1.15, gen->samples / 112.0));
+        forced > 0 ? 1.0 : std::min(2.0, std::max(1.08, gen->samples / 120.0));
     for (uint32_t r0 = 0; r0 < length;) {
       const uint64_t limit = static_cast<uint64_t>(rows[r0]) + cur;
       uint32_t r1 = static_cast<uint32_t>(
