@@ -100,6 +100,9 @@ __device__ __forceinline__ void wmh_update(float t, float r, float c, float b, u
 __device__ __forceinline__ uint2 resolve(const HashArgs &a, uint32_t pos, uint32_t s) {
   if (pos == kNone) return make_uint2(kNone, kNone);
   const uint32_t k = a.cols[pos];
+  // An invalid column was evaluated as column 0 and failed the call: keep
+  // the parameter reads in bounds.
+  if (k >= a.dim) return make_uint2(kNone, kNone);
   const float w = logf(a.weights[pos]);
   const float *col = a.params + static_cast<size_t>(k) * 3 * a.s_pad + s;
   const float t = exact_t(w, col[0], col[2 * static_cast<size_t>(a.s_pad)]);
@@ -243,9 +246,12 @@ __device__ __forceinline__ void issue_window(const HashArgs &a, WarpStage &st, u
   }
 }
 
-// Waits for buffer `b` (bounded), loads the tail, and turns weights into
-// ln(weight) in place -- once per nnz, lane-parallel.  Returns false if the
-// copy did not complete within the spin limit.
+// Waits for buffer `b` (bounded), loads the tail, turns weights into
+// ln(weight) in place -- once per nnz, lane-parallel -- and validates the
+// columns: a column >= dim flags kStatusBadColumn (the call then fails, its
+// hashes are not valid output) and is replaced by column 0, so the
+// evaluation loop reads only in-bounds parameters without a check per nnz.
+// Returns false if the copy did not complete within the spin limit.
 __device__ __forceinline__ bool finish_window(const HashArgs &a, WarpStage &st, uint32_t b,
                                               uint32_t parity, uint32_t ws, uint32_t n,
                                               bool bulk_ok, uint32_t lane) {
@@ -254,19 +260,28 @@ __device__ __forceinline__ bool finish_window(const HashArgs &a, WarpStage &st, 
     if (++spins > kSpinLimit) return false;
   }
   const uint32_t nb = bulk_ok ? (n & ~3u) : 0u;
+  bool bad = false;
   for (uint32_t i = lane; i < n; i += 32) {
     float x;
+    uint32_t col;
     if (i < nb) {
       x = st.w[b][i];
+      col = st.c[b][i];
     } else if (a.host_csr) {  // mapped host memory: plain loads
       x = a.weights[ws + i];
-      st.c[b][i] = a.cols[ws + i];
+      col = a.cols[ws + i];
     } else {
       x = __ldg(a.weights + ws + i);
-      st.c[b][i] = __ldg(a.cols + ws + i);
+      col = __ldg(a.cols + ws + i);
     }
+    if (col >= a.dim) {
+      bad = true;
+      col = 0;
+    }
+    st.c[b][i] = col;
     st.w[b][i] = logf(x);
   }
+  if (__any_sync(0xFFFFFFFFu, bad) && lane == 0) atomicOr(a.status, kStatusBadColumn);
   __syncwarp();
   return true;
 }
@@ -476,9 +491,10 @@ __global__ void __launch_bounds__(kHashBlock, MINB) hash_kernel(const HashArgs a
       const float *__restrict__ lw = stg.w[b];
       const uint32_t *__restrict__ cl = stg.c[b];
 
+      // Columns in the window are < dim (finish_window).
       Params<SPL> A, B;
       uint32_t dA = cl[0], dB = 0;
-      if (active && dA < a.dim) A.load(pbase + dA * col_stride, a.s_pad);
+      if (active) A.load(pbase + dA * col_stride, a.s_pad);
       uint32_t i = 0;
       while (i < n) {
         // Row boundaries (warp-uniform): finish rows, start the next owned one.
@@ -499,24 +515,21 @@ __global__ void __launch_bounds__(kHashBlock, MINB) hash_kernel(const HashArgs a
         // evaluated, A for i+2 while B is evaluated.
         while (i + 1 < seg) {
           dB = cl[i + 1];
-          if (active && dB < a.dim) B.load(pbase + dB * col_stride, a.s_pad);
-          if (dA < a.dim) eval_all<SPL>(A, lw[i], ws + i, active, st);
-          else if (lane == 0) atomicOr(a.status, kStatusBadColumn);
+          if (active) B.load(pbase + dB * col_stride, a.s_pad);
+          eval_all<SPL>(A, lw[i], ws + i, active, st);
           if (i + 2 < n) {
             dA = cl[i + 2];
-            if (active && dA < a.dim) A.load(pbase + dA * col_stride, a.s_pad);
+            if (active) A.load(pbase + dA * col_stride, a.s_pad);
           }
-          if (dB < a.dim) eval_all<SPL>(B, lw[i + 1], ws + i + 1, active, st);
-          else if (lane == 0) atomicOr(a.status, kStatusBadColumn);
+          eval_all<SPL>(B, lw[i + 1], ws + i + 1, active, st);
           i += 2;
         }
         if (i < seg) {
           if (i + 1 < n) {
             dB = cl[i + 1];
-            if (active && dB < a.dim) B.load(pbase + dB * col_stride, a.s_pad);
+            if (active) B.load(pbase + dB * col_stride, a.s_pad);
           }
-          if (dA < a.dim) eval_all<SPL>(A, lw[i], ws + i, active, st);
-          else if (lane == 0) atomicOr(a.status, kStatusBadColumn);
+          eval_all<SPL>(A, lw[i], ws + i, active, st);
           ++i;
           A = B;
           dA = dB;
