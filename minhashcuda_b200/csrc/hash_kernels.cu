@@ -175,10 +175,13 @@ constexpr uint32_t kWin = 256;  // CSR positions per staged window
 constexpr uint32_t kSpinLimit = 1u << 22;
 
 // One warp's staging area: two windows of weights (turned into ln w in
-// place) and column indices, each with its own transaction barrier.
+// place) and column indices, each with its own transaction barrier.  Column
+// slot n of a window of n positions holds column 0, so the loop may prefetch
+// one position past the window without a bounds branch (the row stride of c,
+// kWin + 4 words, keeps both windows 16-byte aligned for the bulk copies).
 struct alignas(16) WarpStage {
   float w[2][kWin];
-  uint32_t c[2][kWin];
+  uint32_t c[2][kWin + 4];
   unsigned long long bar[2];
 };
 
@@ -282,6 +285,7 @@ __device__ __forceinline__ bool finish_window(const HashArgs &a, WarpStage &st, 
     st.w[b][i] = logf(x);
   }
   if (__any_sync(0xFFFFFFFFu, bad) && lane == 0) atomicOr(a.status, kStatusBadColumn);
+  if (lane == 0) st.c[b][n] = 0;  // the prefetch slot past the window
   __syncwarp();
   return true;
 }
@@ -431,7 +435,9 @@ __global__ void __launch_bounds__(kHashBlock, MINB) hash_kernel(const HashArgs a
     const uint32_t tile = item - c * a.ntiles;
     const uint32_t s0 = tile * (32u * SPL) + lane * SPL;
     const bool active = s0 < a.s_pad;
-    const float *__restrict__ pbase = a.params + s0;
+    // Lanes past the last sample read the tile's first samples (in bounds)
+    // and never store, so parameter loads need no branch.
+    const float *__restrict__ pbase = a.params + (active ? s0 : tile * (32u * SPL));
     const uint32_t cs = c * a.chunk;
     const uint32_t ce = cs + min(a.chunk, a.nnz - cs);  // no uint32 overflow near 2^32
     uint32_t r_next = a.chunk_row[c];
@@ -491,10 +497,11 @@ __global__ void __launch_bounds__(kHashBlock, MINB) hash_kernel(const HashArgs a
       const float *__restrict__ lw = stg.w[b];
       const uint32_t *__restrict__ cl = stg.c[b];
 
-      // Columns in the window are < dim (finish_window).
+      // Columns in the window are < dim, and slot n holds column 0
+      // (finish_window).
       Params<SPL> A, B;
       uint32_t dA = cl[0], dB = 0;
-      if (active) A.load(pbase + dA * col_stride, a.s_pad);
+      A.load(pbase + dA * col_stride, a.s_pad);
       uint32_t i = 0;
       while (i < n) {
         // Row boundaries (warp-uniform): finish rows, start the next owned one.
@@ -513,22 +520,18 @@ __global__ void __launch_bounds__(kHashBlock, MINB) hash_kernel(const HashArgs a
         const uint32_t seg = min(row_end - ws, n);
         // Pairs: A holds position i, B is loaded for i+1 while A is
         // evaluated, A for i+2 while B is evaluated.
-        while (i + 1 < seg) {
+        while (i + 1 < seg) {  // i + 2 <= n
           dB = cl[i + 1];
-          if (active) B.load(pbase + dB * col_stride, a.s_pad);
+          B.load(pbase + dB * col_stride, a.s_pad);
           eval_all<SPL>(A, lw[i], ws + i, active, st);
-          if (i + 2 < n) {
-            dA = cl[i + 2];
-            if (active) A.load(pbase + dA * col_stride, a.s_pad);
-          }
+          dA = cl[i + 2];
+          A.load(pbase + dA * col_stride, a.s_pad);
           eval_all<SPL>(B, lw[i + 1], ws + i + 1, active, st);
           i += 2;
         }
-        if (i < seg) {
-          if (i + 1 < n) {
-            dB = cl[i + 1];
-            if (active) B.load(pbase + dB * col_stride, a.s_pad);
-          }
+        if (i < seg) {  // i + 1 <= n
+          dB = cl[i + 1];
+          B.load(pbase + dB * col_stride, a.s_pad);
           eval_all<SPL>(A, lw[i], ws + i, active, st);
           ++i;
           A = B;
