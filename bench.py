@@ -9,7 +9,11 @@ steps.
 
   value  device throughput: the CSR is resident in HBM, one step is one
          mhcuda_calc_device call (plan + hash + finalize kernels), timed with
-         CUDA events on the launch stream.
+         CUDA events on the launch stream.  Before warm-up, mhcuda_autotune
+         picks the kernel variant for this data (samples per lane, register
+         budget, chunk granularity; results never depend on it) and the line
+         reports its choice under "autotuned" (--no-autotune: the planner's
+         default).
   e2e    the same metric through the drop-in C ABI call mhcuda_calc with
          pinned host buffers: every step copies the CSR host->device and the
          hashes device->host inside the timed region.
@@ -26,9 +30,10 @@ implementation of the hash (kernel.cu is CUDA only), so it times the C oracle
 port of the reference kernel on all host cores over a bounded sample of the
 same workload per step.
 
-Multi-GPU: the path has no exchange step; N ranks run N independent replicas
-(weak scaling, one process per GPU, no data-path collective).  Timing is the
-max over ranks of the per-rank device time.
+Multi-GPU: the path has no exchange step; N ranks run N independent replicas,
+rank r on rows [r*R, (r+1)*R) of the seeded workload (weak scaling, one
+process per GPU, no data-path collective).  Timing is the max over ranks of
+the per-rank device time; the job's evals are summed over ranks.
 """
 from __future__ import annotations
 
@@ -711,8 +716,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-rows", type=int, default=3000)
-    ap.add_argument("--autotune", action="store_true",
-                    help="pick the hash kernel variant with mhcuda_autotune before timing")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="time the planner's default kernel variant instead of the one "
+                         "mhcuda_autotune picks for this data before the timed region")
     args = ap.parse_args()
 
     rank, world, local = dist_setup()
