@@ -1,7 +1,7 @@
 """Python handle on the continuous-batching server (mhcuda_server_* in
 include/minhashcuda_b200.h).
 
-    srv = Server(hbm_budget=8 << 30, lanes=4)
+    srv = Server(hbm_budget=8 << 30, lanes=8)
     t = srv.submit(gen, csr)          # gen: handle from libMHCUDA.minhash_cuda_init
     hashes = srv.wait(t)              # (rows, samples, 2) uint32, as minhash_cuda_calc
     srv.stop()
@@ -19,8 +19,11 @@ from . import MHCUDAError, RUNTIME_ERROR, capi, check
 
 
 class Server:
-    def __init__(self, hbm_budget: int = 8 << 30, lanes: int = 4, devices: int = 0,
+    def __init__(self, hbm_budget: int = 8 << 30, lanes: int = 8, devices: int = 0,
                  verbosity: int = 0):
+        """Starts a server on one device.  Two of the `lanes` are kept for small
+        requests (at most lanes - 2 large batches are out at once); the device
+        memory used is `hbm_budget` bytes, split between the lanes."""
         self._lib = capi()
         status = ctypes.c_int(-1)
         self._h = self._lib.mhcuda_server_start(devices, int(hbm_budget), lanes, verbosity,
