@@ -16,14 +16,17 @@
 //    32*SPL samples are three fully coalesced warp loads (SPL=4: 3 x 512 B),
 //  - a warp owns one (chunk, sample tile) item; each lane keeps SPL running
 //    minima in registers (no shared-memory spill as in kernel.cu:72-74),
+//    each with the position of its entry; (k, t) are recovered once per
+//    (row, sample) at the row's end,
 //  - each warp stages its CSR positions in 256-entry windows with TMA bulk
 //    copies (cp.async.bulk, mbarrier completion, double-buffered), turns the
 //    weights into ln(weight) in place once per nnz, lane-parallel (the
-//    reference evaluates logf once per thread, :95), and reads them back as
-//    shared-memory broadcasts,
+//    reference evaluates logf once per thread, :95), validates the window's
+//    columns once, and reads them back as shared-memory broadcasts,
 //  - parameters for the next nnz are loaded into a second register set while
-//    the current one is evaluated (ping-pong, no register copies), and the
-//    running minimum is updated with selects instead of branches,
+//    the current one is evaluated (ping-pong, no register copies); the loop
+//    has no branch per nnz, samples are evaluated in pairs with packed f32x2
+//    arithmetic, and the running minimum is updated with selects,
 //  - work is cut by nnz, not by rows, so one 50k-nnz row and many 5-nnz rows
 //    cost the same per item; rows that cross a chunk boundary are merged by
 //    a finalize pass (tie -> earlier position, as the strict '<' scan).
