@@ -131,6 +131,81 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+KERNEL_SOURCE = os.path.join(ROOT, "minhashcuda_b200", "csrc", "hash_kernels.cu")
+PROFILE_JSON = os.path.join(ROOT, "profiles", "hash_kernel_traffic.json")
+SMS = 148
+ISSUE_PER_SM_CLK = 4 * 32  # four schedulers, one warp-instruction (32 threads) per clock each
+
+
+def kernel_source_sha16():
+    import hashlib
+    with open(KERNEL_SOURCE, "rb") as f:
+        return hashlib.sha256(f.read()).hexdigest()[:16]
+
+
+def kernel_profile():
+    """Counters ncu measured for the hash kernel on a 20,000-row case of the
+    large workload (profiles/hash_kernel_traffic.json), and whether they were
+    taken on the kernel source this run built."""
+    if not os.path.exists(PROFILE_JSON):
+        return None, False
+    d = json.load(open(PROFILE_JSON))
+    return d, d.get("source_sha16") == kernel_source_sha16()
+
+
+def digest(a):
+    import hashlib
+    return hashlib.sha1(np.ascontiguousarray(a).tobytes()).hexdigest()[:16]
+
+
+def hash_roofline(nnz, R, S, kernel_ms, sm_mhz, peak, peak_kind, profile, profile_current):
+    """Roofline of one hash launch.  Three bounds are reported side by side:
+    DRAM traffic (ncu bytes per eval of this workload, scaled to the launch)
+    over the measured HBM bandwidth; issue (ncu thread-instructions per eval
+    over 148 SMs x 128 thread-instructions per clock at the run's median SM
+    clock); and the FP32 issue floor of 8 operations per eval.  `bound` is the
+    one closest to its peak; the algorithmic bytes 12NS + 8N + 4(R+1) + 8RS
+    are kept beside them (their rate exceeds HBM when hot columns hit L2)."""
+    t = kernel_ms / 1e3
+    evals = nnz * S
+    alg = 12 * nnz * S + 8 * nnz + 4 * (R + 1) + 8 * R * S
+    out = {"kernel": "hash_kernel", "kernel_ms": kernel_ms, "algorithmic_bytes": alg,
+           "algorithmic_gbs": alg / t / 1e9, "algorithmic_frac": alg / t / 1e9 / peak,
+           "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)", "sm_mhz": sm_mhz}
+    cands = {}
+    traffic = None
+    if profile and profile.get("dram_bytes_per_eval"):
+        traffic = profile["dram_bytes_per_eval"] * evals
+        gbs = traffic / t / 1e9
+        out["dram"] = {"achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+                       "bytes_per_eval": profile["dram_bytes_per_eval"]}
+        cands["hbm"] = out["dram"]
+    if sm_mhz:
+        issue_peak = SMS * ISSUE_PER_SM_CLK * sm_mhz * 1e6 / 1e12
+        if profile and profile.get("thread_inst_per_eval"):
+            ach = profile["thread_inst_per_eval"] * evals / t / 1e12
+            out["issue"] = {"achieved": ach, "peak": issue_peak, "unit": "T thread-inst/s",
+                            "frac": ach / issue_peak,
+                            "inst_per_eval": profile["thread_inst_per_eval"]}
+            cands["issue"] = out["issue"]
+        fp = 8 * evals / t / 1e12
+        out["fp32_floor"] = {"achieved": fp, "peak": issue_peak, "unit": "T ops/s",
+                             "frac": fp / issue_peak, "ops_per_eval": 8}
+    out["profile"] = {"source": os.path.relpath(PROFILE_JSON, ROOT),
+                      "case": profile.get("captured_case") if profile else None,
+                      "matches_built_kernel": profile_current}
+    if cands:
+        bound = max(cands, key=lambda k: cands[k]["frac"])
+        b = cands[bound]
+        out.update({"bound": bound, "achieved": b["achieved"], "peak": b["peak"],
+                    "unit": b["unit"], "frac": b["frac"]})
+    else:
+        out.update({"bound": "hbm", "achieved": alg / t / 1e9, "peak": peak, "unit": "GB/s",
+                    "frac": alg / t / 1e9 / peak})
+    out["traffic"] = traffic
+    return out
+
+
 def cpu_oracle_sample(w, params_host, target_s=12.0, check=None, nthreads=0, max_rows=20000):
     """Times the C oracle on the first rows of the workload, growing the
     sample until it takes ~target_s.  Returns (evals/s, rows, nnz, seconds,
@@ -199,19 +274,172 @@ def run_reference_arm(args, rank):
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "rows_per_s": rows / t,
     }
+    del co
+    if args.extras and args.gpus == 1:
+        line["reference_cuda"] = reference_cuda_cases()
     print(json.dumps(line), flush=True)
 
 
-def run_batched(args, rank, world, local):
+def reference_cuda_cases():
+    """The reference's own CUDA implementation, compiled from its sources for
+    sm_100a (oracle/_ref/libMHCUDA.so, oracle/Makefile), timed through its C
+    ABI on the inputs the default arm times this engine on
+    (`same_inputs_as_reference_cuda`); equal digests mean bit-identical
+    hashes."""
+    path = os.path.join(ROOT, "oracle", "_ref", "libMHCUDA.so")
+    if not os.path.exists(path):
+        return {"unavailable": "oracle/_ref/libMHCUDA.so was not built (no reference sources)"}
+    lib = ctypes.CDLL(path)
+    Pt, U32 = ctypes.c_void_p, ctypes.c_uint32
+    lib.mhcuda_init.restype = Pt
+    lib.mhcuda_init.argtypes = [U32, ctypes.c_uint16, U32, ctypes.c_int, U32, ctypes.c_int,
+                                ctypes.POINTER(ctypes.c_int)]
+    lib.mhcuda_calc.restype = ctypes.c_int
+    lib.mhcuda_calc.argtypes = [Pt, Pt, Pt, Pt, U32, Pt]
+    lib.mhcuda_fini.restype = ctypes.c_int
+    lib.mhcuda_fini.argtypes = [Pt]
+    try:
+        res = time_reference_cases(lib, 0)
+    except Exception as e:  # recorded; the CPU arm's value stands
+        return {"error": f"{type(e).__name__}: {e}"}
+    res["build"] = "reference kernel.cu/minhashcuda.cc compiled for sm_100a (oracle/Makefile ref)"
+    return res
+
+
+def _free_cuda():
+    import gc
+    import torch
+    gc.collect()
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+
+
+def extra_uniform(lib, local, peak, peak_kind):
+    """HBM roofline on uniform columns: one 524,288-row block of the streamed
+    workload (12,000,000 dims x 128 samples, 18.4 GB of parameters, uniform
+    columns, so the gathers find nothing in L2), device-resident, one
+    mhcuda_calc_device per step, the hash kernel timed with the events the
+    library records around it."""
+    import torch
+    from minhashcuda_b200 import synth
+    w = synth.WORKLOADS["streamed"]
+    rows, S = w.extra["block_rows"], w.samples
+    st = ctypes.c_int(-1)
+    gen = lib.mhcuda_init(w.dim, S, w.seed, 0, 1 << local, 0, ctypes.byref(st))
+    assert gen, st.value
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        ip, cols, wts, nnz = synth.device_csr(w, 0, rows, stream=stream)
+    out = torch.empty((rows, S, 2), dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    sp = ctypes.c_void_p(stream.cuda_stream)
+
+    def step():
+        assert lib.mhcuda_calc_device(gen, wts.data_ptr(), cols.data_ptr(), ip.data_ptr(), rows,
+                                      nnz, out.data_ptr(), sp) == 0
+
+    for _ in range(3):
+        step()
+    lib.mhcuda_profile(gen, 1)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(5):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    hm, nl = ctypes.c_double(0), ctypes.c_uint64(0)
+    assert lib.mhcuda_profile_read(gen, ctypes.byref(hm), ctypes.byref(nl)) == 0
+    lib.mhcuda_profile(gen, 0)
+    assert lib.mhcuda_device_status(gen) == 0
+    lib.mhcuda_fini(gen)
+    kernel_ms = hm.value / max(1, nl.value)
+    alg = 12 * nnz * S + 8 * nnz + 4 * (rows + 1) + 8 * rows * S
+    gbs = alg / (kernel_ms / 1e3) / 1e9
+    del ip, cols, wts, out
+    _free_cuda()
+    return {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+            "traffic": None, "kernel": "hash_kernel", "kernel_ms": kernel_ms,
+            "algorithmic_bytes": alg, "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
+            "value": nnz * S / (e0.elapsed_time(e1) / 5 / 1e3), "unit_value": UNIT,
+            "workload": f"streamed block: {rows} rows x {w.dim} dims, {S} samples, {nnz} nnz, "
+                        "uniform columns, device-resident"}
+
+
+def _time_host_calls(lib, gen, calls, S, reps, warmup=1):
+    """Times `reps` passes over `calls` [(weights, cols, indptr)] through the
+    C ABI mhcuda_calc with pageable numpy buffers (the reference's calling
+    convention); returns (seconds per pass, outputs of the last pass)."""
+    outs = [np.empty((len(ip) - 1, S, 2), np.uint32) for _, _, ip in calls]
+
+    def one():
+        for (wt, cl, ip), o in zip(calls, outs):
+            rc = lib.mhcuda_calc(gen, wt.ctypes.data, cl.ctypes.data, ip.ctypes.data,
+                                 len(ip) - 1, o.ctypes.data)
+            assert rc == 0, rc
+
+    for _ in range(warmup):
+        one()
+    t = time.perf_counter()
+    for _ in range(reps):
+        one()
+    return (time.perf_counter() - t) / reps, outs
+
+
+def reference_cases():
+    """Inputs the reference CUDA build (in the reference arm) and this engine
+    (in the default arm) both hash through their own C ABI, mhcuda_calc, with
+    pageable numpy buffers, for a same-box comparison: name -> (dim, samples,
+    seed, calls, reps)."""
+    from minhashcuda_b200 import synth
+    cases = {}
+    ip, cl, wt = synth.small_csr(1)
+    cases["small_6400x130"] = (130, 128, 1, [(wt, cl, ip)], 20)
+    w = synth.WORKLOADS["large"]
+    ip, cl, wt = synth.host_csr(w, 0, 200_000)
+    cases["large_first_200000_rows"] = (w.dim, w.samples, w.seed, [(wt, cl, ip)], 2)
+    w = synth.WORKLOADS["batched"]
+    shapes = synth.batched_shapes(w)[:512]
+    ip, cl, wt = synth.host_csr(w, 0, int(shapes.sum()))
+    base = np.concatenate([[0], np.cumsum(shapes)])
+    calls = [(wt, cl, ip[base[i]:base[i + 1] + 1]) for i in range(len(shapes))]
+    cases["batched_first_512_matrices"] = (w.dim, w.samples, w.seed, calls, 1)
+    return cases
+
+
+def time_reference_cases(lib, local):
+    """Times every reference case through `lib`'s mhcuda_calc; each entry
+    carries evals/s and a digest of the hashes (equal digests in the two arms
+    mean bit-identical output)."""
+    res = {}
+    for name, (dim, S, seed, calls, reps) in reference_cases().items():
+        st = ctypes.c_int(-1)
+        gen = lib.mhcuda_init(dim, S, seed, 0, 1 << local, 0, ctypes.byref(st))
+        assert gen, f"mhcuda_init failed: {st.value}"
+        t, outs = _time_host_calls(lib, gen, calls, S, reps)
+        lib.mhcuda_fini(gen)
+        nnz = sum(int(ip[-1]) - int(ip[0]) for _, _, ip in calls)
+        rows = sum(len(ip) - 1 for _, _, ip in calls)
+        res[name] = {"value": nnz * S / t, "unit": UNIT, "ms_per_pass": t * 1e3,
+                     "calls_per_pass": len(calls), "rows": rows, "nnz": nnz, "samples": S,
+                     "digest": digest(np.concatenate([o.reshape(-1) for o in outs]))}
+    return res
+
+
+def run_batched(args, rank, world, local, emit=True, steps=None, warmup=None):
     """The uneven-batch configuration: 4096 CSR matrices sharing one generator
     (2^20 dims, 256 samples), rows per matrix log-uniform in [1, 4096], row
     nnz lognormal(median 64, sigma 1.5) clipped to [1, 20000], uniform
-    columns, lognormal values.  Plain = one mhcuda_calc per matrix; batched =
-    one mhcuda_calc_batch over all of them.  Both through the C ABI with
-    pageable host buffers (inputs in, hashes out, every step)."""
+    columns, lognormal values.  Three ways through the C ABI:
+      plain    one mhcuda_calc per matrix, pageable host buffers in and out;
+      batched  one mhcuda_calc_batch over all of them, same host buffers;
+      device   one mhcuda_calc_batch_device with the matrices resident in
+               device memory (each starting on a 16-byte boundary), outputs
+               left there; repeated calls replay its CUDA graph."""
     import torch
     import minhashcuda_b200 as mb
     from minhashcuda_b200 import synth
+    steps = steps or args.steps
+    warmup = warmup if warmup is not None else args.warmup
     torch.cuda.set_device(local)
     w = synth.WORKLOADS["batched"]
     shapes = synth.batched_shapes(w)
@@ -240,6 +468,29 @@ def run_batched(args, rank, world, local):
     Op = (P * n)(*[out_batch.ctypes.data + row_bytes * int(b) for b in base[:-1]])
     Opl = [out_plain.ctypes.data + row_bytes * int(b) for b in base[:-1]]
 
+    # Device-resident copy: matrix i's entries start on a 16-byte boundary of
+    # one buffer; its offsets are the absolute ones of the host arrays.
+    starts = ip[base[:-1]].astype(np.int64)
+    counts = ip[base[1:]].astype(np.int64) - starts
+    padded = np.zeros(n + 1, np.int64)
+    np.cumsum((counts + 3) // 4 * 4, out=padded[1:])
+    src_idx = np.concatenate([np.arange(a, a + c) for a, c in zip(starts, counts)])
+    dst_idx = np.concatenate([np.arange(p, p + c) for p, c in zip(padded[:-1], counts)])
+    d_w = torch.zeros(int(padded[-1]) + 4, dtype=torch.float32, device="cuda")
+    d_c = torch.zeros(int(padded[-1]) + 4, dtype=torch.int32, device="cuda")
+    d_w[torch.from_numpy(dst_idx).cuda()] = torch.from_numpy(wts[src_idx]).cuda()
+    d_c[torch.from_numpy(dst_idx).cuda()] = torch.from_numpy(cols[src_idx].view(np.int32)).cuda()
+    del src_idx, dst_idx
+    d_ip = torch.from_numpy(ip.view(np.int32)).cuda()
+    d_out = torch.empty((total_rows, S, 2), dtype=torch.int32, device="cuda")
+    DW = (P * n)(*[d_w.data_ptr() + 4 * int(p) for p in padded[:-1]])
+    DC = (P * n)(*[d_c.data_ptr() + 4 * int(p) for p in padded[:-1]])
+    DR = (P * n)(*[d_ip.data_ptr() + 4 * int(b) for b in base[:-1]])
+    DO = (P * n)(*[d_out.data_ptr() + row_bytes * int(b) for b in base[:-1]])
+    stream = torch.cuda.Stream()
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    torch.cuda.synchronize()
+
     def plain():
         for i in range(n):
             rc = lib.mhcuda_calc(gen, wts.ctypes.data, cols.ctypes.data, Rp[i], int(shapes[i]),
@@ -250,12 +501,16 @@ def run_batched(args, rank, world, local):
         rc = lib.mhcuda_calc_batch(gen, n, Wp, Cp, Rp, Lp, Op)
         assert rc == 0, rc
 
+    def device():
+        rc = lib.mhcuda_calc_batch_device(gen, n, DW, DC, DR, Lp, DO, sp)
+        assert rc == 0, rc
+
     def timed(fn):
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             fn()
         torch.cuda.synchronize()
         ts = []
-        for _ in range(args.steps):
+        for _ in range(steps):
             t = time.perf_counter()
             fn()
             ts.append(time.perf_counter() - t)
@@ -264,28 +519,46 @@ def run_batched(args, rank, world, local):
     with Clocks(local) as clk:
         t_plain = timed(plain)
         t_batch = timed(batched)
+        for _ in range(max(2, warmup)):  # eager, then captured
+            device()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            device()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t_dev = e0.elapsed_time(e1) / steps / 1e3
+    assert lib.mhcuda_device_status(gen) == 0
     exact = bool(np.array_equal(out_plain, out_batch))
+    exact_dev = bool(np.array_equal(out_plain, d_out.cpu().numpy().view(np.uint32)))
     lib.mhcuda_fini(gen)
+    del d_w, d_c, d_ip, d_out
+    _free_cuda()
     evals = nnz * S
-    if rank == 0:
-        line = {
-            "metric": "WMH nnz*samples/s (batched: 4096 uneven CSR, one call)",
-            "value": evals / t_batch, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": t_batch * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded, generated on the device, copied to pageable host arrays)",
-            "config": {"workload": f"batched: {n} matrices, {total_rows} rows, {nnz} nnz, "
-                                   f"{w.dim} dims, {S} samples", "matrices": n,
-                       "rows": total_rows, "nnz": nnz, "dim": w.dim, "samples": S},
-            "plain": {"value": evals / t_plain, "unit": UNIT, "ms_per_step": t_plain * 1e3,
-                      "calls_per_step": n},
-            "batched_over_plain": t_plain / t_batch, "bit_exact_plain_vs_batched": exact,
-            "rows_per_s": total_rows / t_batch, "clocks": clk.summary(),
-            "e2e": {"value": evals / t_batch, "unit": UNIT,
-                    "h2d_bytes_per_step": 8 * nnz + 4 * total_rows,
-                    "d2h_bytes_per_step": total_rows * row_bytes},
-        }
+    line = {
+        "metric": "WMH nnz*samples/s (batched: 4096 uneven CSR, one call)",
+        "value": evals / t_batch, "unit": UNIT, "n_gpus": world, "steps": steps,
+        "warmup": warmup, "ms_per_step": t_batch * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded, generated on the device, copied to pageable host arrays)",
+        "config": {"workload": f"batched: {n} matrices, {total_rows} rows, {nnz} nnz, "
+                               f"{w.dim} dims, {S} samples", "matrices": n,
+                   "rows": total_rows, "nnz": nnz, "dim": w.dim, "samples": S},
+        "plain": {"value": evals / t_plain, "unit": UNIT, "ms_per_step": t_plain * 1e3,
+                  "calls_per_step": n},
+        "device_resident": {"value": evals / t_dev, "unit": UNIT, "ms_per_step": t_dev * 1e3,
+                            "call": "mhcuda_calc_batch_device (CUDA graph replay)",
+                            "over_plain": t_plain / t_dev},
+        "batched_over_plain": t_plain / t_batch, "bit_exact_plain_vs_batched": exact,
+        "bit_exact_plain_vs_device_batch": exact_dev,
+        "rows_per_s": total_rows / t_batch, "clocks": clk.summary(),
+        "e2e": {"value": evals / t_batch, "unit": UNIT,
+                "h2d_bytes_per_step": 8 * nnz + 4 * total_rows,
+                "d2h_bytes_per_step": total_rows * row_bytes},
+    }
+    if emit and rank == 0:
         print(json.dumps(line), flush=True)
+    return line
 
 
 def run_ingest(args, rank, world, local):
@@ -366,7 +639,7 @@ def run_ingest(args, rank, world, local):
         print(json.dumps(line), flush=True)
 
 
-def run_streamed(args, rank, world, local):
+def run_streamed(args, rank, world, local, emit=True, passes=None):
     """Row-streamed wide generator: 12,000,000 dims x 128 samples (18.4 GB of
     parameters resident), 10,000,000 rows hashed as 19 blocks of 524,288 rows
     plus one of 38,528, each block an mhcuda_calc call on page-locked host
@@ -421,7 +694,7 @@ def run_streamed(args, rank, world, local):
     # is ~1.4 s of host<->device traffic, exposed to other users of the host).
     passes = []
     with Clocks(local) as clk:
-        for _ in range(max(1, args.steps)):
+        for _ in range(max(1, passes or args.steps)):
             t = time.perf_counter()
             evals = sum(run_block(k, rows) for k, rows in schedule)
             passes.append(time.perf_counter() - t)
@@ -450,7 +723,9 @@ def run_streamed(args, rank, world, local):
     run_block(0, block_rows)
     same = bool(np.array_equal(out, d_o.cpu().numpy().view(np.uint32)))
     lib.mhcuda_fini(gen)
-    if rank == 0:
+    del d_ip, d_c, d_w, d_o, blocks, out_t, out
+    _free_cuda()
+    if True:
         nnz_total = evals // S
         line = {
             "metric": "WMH nnz*samples/s (row-streamed: 10M rows x 12M dims, 128 samples)",
@@ -471,7 +746,9 @@ def run_streamed(args, rank, world, local):
                     "h2d_bytes_per_step": int(8 * nnz_total / len(schedule)),
                     "d2h_bytes_per_step": int(w.rows * S * 8 / len(schedule))},
         }
-        print(json.dumps(line), flush=True)
+        if emit and rank == 0:
+            print(json.dumps(line), flush=True)
+        return line
 
 
 def srpt_ideal(sizes, rate, load, seed):
@@ -508,7 +785,7 @@ def srpt_ideal(sizes, rate, load, seed):
     return {"p50_ms": float(p50), "p99_ms": float(p99), "p999_ms": float(p999)}
 
 
-def run_serving(args, rank, world, local):
+def run_serving(args, rank, world, local, emit=True, seconds=None):
     """Serving: Poisson-arriving requests over three resident generators
     (2^20 dims / 128 samples, 2^22 / 64, 2^24 / 256; 1.6 + 3.2 + 51.5 GB of
     parameters), each request a CSR of log-uniform 1..50,000 rows with
@@ -614,7 +891,7 @@ def run_serving(args, rank, world, local):
     levels = []
     for frac in args.serving_loads:
         lam = frac * peak / mean_evals
-        duration = args.serving_seconds
+        duration = seconds or args.serving_seconds
         arrivals = np.cumsum(rng.exponential(1.0 / lam, int(lam * duration * 1.2) + 10))
         arrivals = arrivals[arrivals < duration]
         reqs = [make_req() for _ in arrivals]
@@ -682,13 +959,53 @@ def run_serving(args, rank, world, local):
         "config": {"workload": "serving: generators 2^20/128, 2^22/64, 2^24/256; requests of "
                                "log-uniform 1..50000 rows, row nnz 50*(1+Zipf(2)), Poisson arrivals",
                    "lanes": args.serving_lanes, "hbm_budget_gib": args.serving_budget,
-                   "seconds_per_level": args.serving_seconds},
+                   "seconds_per_level": seconds or args.serving_seconds},
         "saturated_evals_per_s": peak, "mean_evals_per_request": mean_evals,
         "request_evals_p50_p99": [float(x) for x in np.percentile(size_sample, [50, 99])],
         "levels": levels,
         "bit_exact_served_vs_alone": exact,
     }
-    print(json.dumps(line), flush=True)
+    del outs, pools
+    _free_cuda()
+    if emit:
+        print(json.dumps(line), flush=True)
+    return line
+
+
+def run_extras(args, rank, world, local, lib, peak, peak_kind):
+    """The other configurations, measured after the large one on the same
+    GPU, as sub-objects of the one JSON line (each bounded to a few seconds
+    of timed work; an error in one is recorded in its place)."""
+    def summary(line, keys):
+        return {k: line[k] for k in keys if k in line}
+
+    parts = {
+        "roofline_uniform": lambda: extra_uniform(lib, local, peak, peak_kind),
+        "same_inputs_as_reference_cuda": lambda: time_reference_cases(lib, local),
+        "batched": lambda: summary(
+            run_batched(args, rank, world, local, emit=False, steps=2, warmup=1),
+            ["value", "unit", "ms_per_step", "config", "plain", "device_resident",
+             "batched_over_plain", "bit_exact_plain_vs_batched",
+             "bit_exact_plain_vs_device_batch", "rows_per_s", "e2e"]),
+        "streamed": lambda: summary(
+            run_streamed(args, rank, world, local, emit=False, passes=2),
+            ["value", "unit", "config", "rows_per_s", "seconds_total", "pass_seconds",
+             "device_resident", "streamed_equals_device_path", "e2e"]),
+        "serving": lambda: summary(
+            run_serving(args, rank, world, local, emit=False, seconds=3.0),
+            ["metric", "value", "unit", "config", "saturated_evals_per_s", "levels",
+             "bit_exact_served_vs_alone"]),
+    }
+    out = {}
+    for name, fn in parts.items():
+        t = time.perf_counter()
+        try:
+            out[name] = fn()
+        except Exception as e:  # recorded, the main line stands
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+        out[name]["bench_seconds"] = round(time.perf_counter() - t, 1)
+        log(f"[rank {rank}] {name}: {time.perf_counter() - t:.1f}s")
+    return out
 
 
 def workload_config(w, args):
@@ -716,6 +1033,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-rows", type=int, default=3000)
+    ap.add_argument("--no-extras", dest="extras", action="store_false",
+                    help="print only the large configuration (no uniform-column roofline, "
+                         "batched, streamed, serving or same-input sub-objects)")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="time the planner's default kernel variant instead of the one "
                          "mhcuda_autotune picks for this data before the timed region")
@@ -823,19 +1143,10 @@ def main():
     value = job_evals / (ms_step / 1e3)
 
     hash_ms_launch = hash_ms.value / max(1, launches.value)
-    alg_bytes = 12 * nnz * S + 8 * nnz + 4 * (R + 1) + 8 * R * S
     peak, peak_kind = measured_peaks()
-    achieved = alg_bytes / (hash_ms_launch / 1e3) / 1e9
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "hash_kernel_traffic.json")
-    if os.path.exists(tp) and w.name == "large":
-        traffic = json.load(open(tp))["dram_bytes_per_eval"] * evals
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": traffic, "kernel": "hash_kernel",
-                "traffic_source": "profiles/hash_kernel_traffic.json (ncu, 20k-row case, "
-                                  "scaled by evals)" if traffic else None,
-                "kernel_ms": hash_ms_launch, "algorithmic_bytes": alg_bytes,
-                "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)"}
+    prof, prof_current = kernel_profile() if w.name == "large" else (None, False)
+    roofline = hash_roofline(nnz, R, S, hash_ms_launch, clocks.get("sm_mhz"), peak, peak_kind,
+                             prof, prof_current)
 
     # ---- parity spot check + CPU baseline (rank 0) -----------------------------
     cpu = None
@@ -895,7 +1206,10 @@ def main():
                "h2d_bytes_per_step": 8 * nnz + 4 * (R + 1), "d2h_bytes_per_step": 8 * R * S,
                "ms_per_step": e2e_ms, "wall_ms_per_step": wall * 1e3,
                "matches_device_path": same}
+        del h_w, h_c, h_i, h_o
     lib.mhcuda_fini(gen)
+    weights = cols = indptr = out = None  # noqa: F841  (device memory back for the extras)
+    _free_cuda()
 
     if rank == 0:
         line = {
@@ -908,6 +1222,8 @@ def main():
             "parity": parity, "clocks": clocks,
             "gpu_launches": 3 * args.steps, "autotuned": tuned,
         }
+        if world == 1 and args.extras:
+            line.update(run_extras(args, rank, world, local, lib, peak, peak_kind))
         print(json.dumps(line), flush=True)
     if pg:
         pg.barrier()

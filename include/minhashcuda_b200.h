@@ -81,6 +81,28 @@ enum MHCUDAResult mhcuda_calc_device_noalloc(
     const uint32_t *d_cols, const uint32_t *d_rows, uint32_t length,
     uint32_t nnz, uint32_t *d_output, void *stream);
 
+/* Device-resident batch: hashes `count` CSR matrices that already live in
+ * device memory against one generator in one persistent launch, whose warps
+ * take (matrix, chunk of positions, sample tile) items from a table built on
+ * the device.  The five arrays are host arrays of `count` entries; matrix i is
+ * d_weights[i] and d_cols[i] (its entries), d_rows[i] (lengths[i]+1 offsets
+ * whose first value is the offset of d_weights[i][0]) and d_outputs[i]
+ * (lengths[i]*samples*2 uint32), all in the generator's device memory.  A
+ * matrix with lengths[i] == 0 is skipped.  As with mhcuda_calc_device the work
+ * is enqueued on `stream` and the call returns without waiting, calls on one
+ * generator must be ordered on one stream, and invalid CSR content in any
+ * matrix fails the whole batch as reported by the next
+ * mhcuda_device_status().  A batch's descriptors are uploaded to the device
+ * once (the last 8 distinct batches are kept per generator), and a batch
+ * hashed again replays a CUDA graph of its launches.  Results equal one
+ * mhcuda_calc (minhashcuda.h:115-118) per matrix, bit for bit; the reference
+ * has no batch call (one launch per call, minhashcuda.cc:583-642). */
+enum MHCUDAResult mhcuda_calc_batch_device(
+    const MinhashCudaGenerator *gen, uint32_t count,
+    const float *const *d_weights, const uint32_t *const *d_cols,
+    const uint32_t *const *d_rows, const uint32_t *lengths,
+    uint32_t *const *d_outputs, void *stream);
+
 /* Element types accepted by mhcuda_calc_typed. */
 enum MHCUDAElementType {
   mhcudaFloat32 = 0,

@@ -41,6 +41,12 @@ namespace {
 #define MHB_DEBUG(gen, ...) \
   do { if ((gen)->verbosity > 1) { printf(__VA_ARGS__); fflush(stdout); } } while (0)
 
+// Makes the generator's device current until the enclosing function returns
+// (mhb::DeviceGuard), or returns mhcudaNoSuchDevice.
+#define MHB_ON_DEVICE(gen)                                \
+  mhb::DeviceGuard device_guard__((gen)->device);         \
+  if (!device_guard__.ok()) return mhcudaNoSuchDevice
+
 // Returns `code` from the enclosing function when `call` fails.
 #define MHB_CHECK(gen, call, code)                                                  \
   do {                                                                              \
@@ -131,6 +137,23 @@ struct GraphEntry {
   cudaGraphExec_t exec = nullptr;
 };
 
+// A device-resident batch seen by mhcuda_calc_batch_device: its matrix
+// descriptors, copied to the device once, and the CUDA graph of its launches
+// once the same batch has been hashed twice.
+struct BatchEntry {
+  std::vector<unsigned char> key;
+  DevBuf desc;                    // BatchMatrix[count], then plan_base[count]
+  PinnedBuf staging;              // host copy the descriptors were uploaded from
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t used = nullptr;     // after the last launch that read `desc`
+  uint32_t seen = 0;
+  ~BatchEntry() {
+    if (used) cudaEventSynchronize(used);
+    if (exec) cudaGraphExecDestroy(exec);
+    if (used) cudaEventDestroy(used);
+  }
+};
+
 }  // namespace
 
 // The generator.  Opaque to callers (minhashcuda.h declares only the tag).
@@ -172,6 +195,9 @@ struct MinhashCudaGenerator_ {
   mutable std::unordered_map<uint64_t, TuneChoice> tuned;
   // CUDA graphs of mhcuda_calc_device calls, most recent last.
   mutable std::vector<GraphEntry> graphs;
+  // Device-resident batches, most recent last, and their batch-wide scratch.
+  mutable std::vector<std::unique_ptr<BatchEntry>> batches;
+  mutable DevBuf d_chunk_owner, d_batch_plan;
   // Optional timing of every hash-kernel launch with CUDA events recorded on
   // the launch stream (mhcuda_profile / mhcuda_profile_read).
   mutable bool profiling = false;
@@ -179,8 +205,9 @@ struct MinhashCudaGenerator_ {
   mutable size_t prof_used = 0;
 
   ~MinhashCudaGenerator_() {
-    cudaSetDevice(device);
+    mhb::DeviceGuard on_device(device);
     if (stream) cudaStreamSynchronize(stream);
+    batches.clear();  // waits for the launches that read each batch's descriptors
     d_weights.release(); d_cols.release(); d_indptr.release(); d_out.release();
     d_chunk_row.release(); d_part_ln.release(); d_part_kt.release(); d_status.release();
     h_status.release();
@@ -198,6 +225,7 @@ struct MinhashCudaGenerator_ {
     if (s_in) cudaStreamDestroy(s_in);
     if (s_out) cudaStreamDestroy(s_out);
     for (auto &g : graphs) cudaGraphExecDestroy(g.exec);
+    d_chunk_owner.release(); d_batch_plan.release();
     if (params) cudaFree(params);
     if (stream) cudaStreamDestroy(stream);
   }
@@ -237,6 +265,15 @@ uint64_t tune_key(uint64_t nnz, uint64_t rows) {
   return (lg(nnz + 1) << 8) | lg(avg + 1);
 }
 
+// The autotuner's choice for launches of this shape class, if it has one.
+bool tuned_choice(const Gen *gen, uint64_t nnz, uint64_t rows, TuneChoice *out) {
+  std::lock_guard<std::mutex> lock(gen->tune_mu);
+  const auto it = gen->tuned.find(tune_key(nnz, rows));
+  if (it == gen->tuned.end()) return false;
+  *out = it->second;
+  return true;
+}
+
 // min_items: items per resident warp the chunk is capped to give (8 for the
 // engine's own calls; the server asks for 2, its launches overlap).
 HashPlan make_plan(const Gen *gen, uint64_t nnz, uint64_t rows, const TuneChoice *force = nullptr,
@@ -249,12 +286,7 @@ HashPlan make_plan(const Gen *gen, uint64_t nnz, uint64_t rows, const TuneChoice
     tuned = *force;
     have_tuned = true;
   } else {
-    std::lock_guard<std::mutex> lock(gen->tune_mu);
-    const auto it = gen->tuned.find(tune_key(nnz, rows));
-    if (it != gen->tuned.end()) {
-      tuned = it->second;
-      have_tuned = true;
-    }
+    have_tuned = tuned_choice(gen, nnz, rows, &tuned);
   }
   int spl = env_int("MHCUDA_B200_SPL", 0);
   if (have_tuned && spl == 0) spl = static_cast<int>(tuned.spl);
@@ -280,7 +312,7 @@ HashPlan make_plan(const Gen *gen, uint64_t nnz, uint64_t rows, const TuneChoice
   }
   const uint32_t tile_w = 32u * p.spl;
   p.ntiles = (s_pad + tile_w - 1) / tile_w;
-  const int bps = mhb::hash_blocks_per_sm(p.spl, p.minb);
+  const int bps = mhb::hash_blocks_per_sm(p.spl, p.minb, s_pad);
   const uint64_t resident_warps =
       static_cast<uint64_t>(gen->sm_count) * bps * (mhb::kHashBlock / 32);
   const int waves = std::max(
@@ -513,6 +545,11 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
   const size_t row_bytes = static_cast<size_t>(gen->samples) * 2 * sizeof(uint32_t);
   MHB_CHECK(gen, gen->d_status.ensure(sizeof(uint32_t)), mhcudaMemoryAllocationFailure);
   MHB_CHECK(gen, cudaMemsetAsync(gen->d_status.ptr, 0, sizeof(uint32_t), st), mhcudaRuntimeError);
+  // The blocks are cut from one matrix: a variant the autotuner chose for the
+  // whole matrix's shape applies to each of them (their own, smaller shape
+  // classes were never timed).
+  TuneChoice whole{};
+  const TuneChoice *force = tuned_choice(gen, nnz, length, &whole) ? &whole : nullptr;
 
   // Finishes a slot: waits for its hashes and moves staged ones to the caller.
   auto retire = [&](Gen::Slot &sl) -> MHCUDAResult {
@@ -576,7 +613,7 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
       const uint64_t n = static_cast<uint64_t>(rows[b.r1]) - rows[b.r0];
       max_n = std::max(max_n, n);
       max_len = std::max<uint64_t>(max_len, b.r1 - b.r0);
-      max_chunks = std::max(max_chunks, make_plan(gen, n, b.r1 - b.r0).nchunks);
+      max_chunks = std::max(max_chunks, make_plan(gen, n, b.r1 - b.r0, force).nchunks);
     }
     for (int k = 0; k < Gen::kPipeSlots; ++k) {
       Gen::Slot &sl = gen->slots[k];
@@ -639,7 +676,7 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
     }
     MHB_CHECK(gen, cudaEventRecord(sl.h2d, gen->s_in), mhcudaRuntimeError);
     MHB_CHECK(gen, cudaStreamWaitEvent(st, sl.h2d, 0), mhcudaRuntimeError);
-    const HashPlan plan = make_plan(gen, n, len);
+    const HashPlan plan = make_plan(gen, n, len, force);
     HashArgs a{};
     r = prepare_launch(gen, len, n, plan, &a);
     if (r != mhcudaSuccess) break;
@@ -761,6 +798,68 @@ MHCUDAResult init_params(Gen *gen, uint32_t seed) {
 
 namespace mhb {
 
+namespace {
+
+// cuCtxGetCurrent / cuCtxSetCurrent, looked up through the runtime so that
+// the library does not link the driver library directly.
+using CtxGetFn = int (*)(void **);
+using CtxSetFn = int (*)(void *);
+
+struct CtxFns {
+  CtxGetFn get = nullptr;
+  CtxSetFn set = nullptr;
+};
+
+const CtxFns &ctx_fns() {
+  static const CtxFns fns = []() {
+    CtxFns f;
+    void *g = nullptr, *s = nullptr;
+    cudaDriverEntryPointQueryResult qg{}, qs{};
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &g, cudaEnableDefault, &qg) == cudaSuccess &&
+        cudaGetDriverEntryPoint("cuCtxSetCurrent", &s, cudaEnableDefault, &qs) == cudaSuccess &&
+        qg == cudaDriverEntryPointSuccess && qs == cudaDriverEntryPointSuccess) {
+      f.get = reinterpret_cast<CtxGetFn>(g);
+      f.set = reinterpret_cast<CtxSetFn>(s);
+    }
+    cudaGetLastError();
+    return f;
+  }();
+  return fns;
+}
+
+}  // namespace
+
+DeviceGuard::DeviceGuard(int device) {
+  const CtxFns &f = ctx_fns();
+  void *ctx = nullptr;
+  if (f.get && f.get(&ctx) == 0) had_context_ = ctx != nullptr;
+  if (cudaGetDevice(&prev_) != cudaSuccess) {
+    cudaGetLastError();
+    prev_ = -1;
+  }
+  if (prev_ == device && had_context_) {
+    ok_ = true;
+    return;
+  }
+  ok_ = cudaSetDevice(device) == cudaSuccess;
+  if (!ok_) {
+    cudaGetLastError();
+    return;
+  }
+  changed_ = prev_ != device || !had_context_;
+}
+
+DeviceGuard::~DeviceGuard() {
+  if (!changed_) return;
+  const CtxFns &f = ctx_fns();
+  if (!had_context_ && f.set) {
+    f.set(nullptr);
+  } else if (prev_ >= 0) {
+    cudaSetDevice(prev_);
+  }
+  cudaGetLastError();
+}
+
 HashPlan plan_for_generator(const MinhashCudaGenerator_ *gen, uint64_t nnz, uint64_t rows,
                             uint32_t min_items) {
   return make_plan(gen, nnz, rows, nullptr, min_items);
@@ -793,8 +892,12 @@ MinhashCudaGenerator *mhcuda_init(uint32_t dim, uint16_t samples, uint32_t seed,
     return nullptr;
   }
   const int dev = pick_device(devices);
-  if (dev < 0 || cudaSetDevice(dev) != cudaSuccess) {
-    cudaGetLastError();
+  if (dev < 0) {
+    set(mhcudaNoSuchDevice);
+    return nullptr;
+  }
+  mhb::DeviceGuard on_device(dev);
+  if (!on_device.ok()) {
     set(mhcudaNoSuchDevice);
     return nullptr;
   }
@@ -861,7 +964,7 @@ enum MHCUDAResult mhcuda_retrieve_random_vars(const MinhashCudaGenerator *gen, f
                                               float *ln_cs, float *betas) {
   if (!gen || !rs || !ln_cs || !betas) return mhcudaInvalidArguments;
   std::lock_guard<std::mutex> lock(gen->mu);
-  MHB_CHECK(gen, cudaSetDevice(gen->device), mhcudaNoSuchDevice);
+  MHB_ON_DEVICE(gen);
   const uint32_t D = gen->dim, S = gen->samples;
   const uint32_t rows = param_chunk_rows(D, S);
   DevBuf tmp;
@@ -889,7 +992,7 @@ enum MHCUDAResult mhcuda_assign_random_vars(const MinhashCudaGenerator *gen, con
                                             const float *ln_cs, const float *betas) {
   if (!gen || !rs || !ln_cs || !betas) return mhcudaInvalidArguments;
   std::lock_guard<std::mutex> lock(gen->mu);
-  MHB_CHECK(gen, cudaSetDevice(gen->device), mhcudaNoSuchDevice);
+  MHB_ON_DEVICE(gen);
   const uint32_t D = gen->dim, S = gen->samples;
   const uint32_t rows = param_chunk_rows(D, S);
   DevBuf tmp;
@@ -917,7 +1020,7 @@ enum MHCUDAResult mhcuda_calc(const MinhashCudaGenerator *gen, const float *weig
                               uint32_t *output) {
   if (!gen || !weights || !cols || !rows || !output || length == 0) return mhcudaInvalidArguments;
   std::lock_guard<std::mutex> lock(gen->mu);
-  MHB_CHECK(gen, cudaSetDevice(gen->device), mhcudaNoSuchDevice);
+  MHB_ON_DEVICE(gen);
   const uint32_t base = rows[0];
   if (rows[length] < base) return mhcudaInvalidArguments;
   const uint32_t nnz = rows[length] - base;
@@ -1011,7 +1114,7 @@ enum MHCUDAResult mhcuda_calc_typed(const MinhashCudaGenerator *gen, const void 
     return mhcuda_calc(gen, static_cast<const float *>(w), static_cast<const uint32_t *>(c), r32,
                        length, output);
   std::lock_guard<std::mutex> lock(gen->mu);
-  MHB_CHECK(gen, cudaSetDevice(gen->device), mhcudaNoSuchDevice);
+  MHB_ON_DEVICE(gen);
   if (r32[length] < r32[0]) return mhcudaInvalidArguments;
   return calc_pipelined(gen, HostCsr{w, w64, c, cols64, r32}, length, output);
 }
@@ -1023,7 +1126,7 @@ enum MHCUDAResult mhcuda_calc_device(const MinhashCudaGenerator *gen, const floa
   if (!gen || !d_rows || !d_output || length == 0 || (nnz && (!d_weights || !d_cols)))
     return mhcudaInvalidArguments;
   std::lock_guard<std::mutex> lock(gen->mu);
-  MHB_CHECK(gen, cudaSetDevice(gen->device), mhcudaNoSuchDevice);
+  MHB_ON_DEVICE(gen);
   const cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : gen->stream;
   const HashPlan plan = make_plan(gen, nnz, length);
   HashArgs a{};
@@ -1076,6 +1179,163 @@ enum MHCUDAResult mhcuda_calc_device(const MinhashCudaGenerator *gen, const floa
   return mhcudaSuccess;
 }
 
+enum MHCUDAResult mhcuda_calc_batch_device(const MinhashCudaGenerator *gen, uint32_t count,
+                                           const float *const *d_weights,
+                                           const uint32_t *const *d_cols,
+                                           const uint32_t *const *d_rows, const uint32_t *lengths,
+                                           uint32_t *const *d_outputs, void *stream) {
+  if (!gen || (count && (!d_weights || !d_cols || !d_rows || !lengths || !d_outputs)))
+    return mhcudaInvalidArguments;
+  // Host descriptors: the CSR and output of every matrix with rows, and its
+  // first thread in the batch's plan launch (rows + 1 threads per matrix).
+  std::vector<mhb::BatchMatrix> mats(count);
+  std::vector<uint32_t> plan_base(count);
+  uint64_t plan_threads = 0;
+  for (uint32_t m = 0; m < count; ++m) {
+    mhb::BatchMatrix &d = mats[m];
+    d = mhb::BatchMatrix{};
+    plan_base[m] = static_cast<uint32_t>(std::min<uint64_t>(plan_threads, 0xFFFFFFFFull));
+    if (!lengths[m]) continue;
+    if (!d_weights[m] || !d_cols[m] || !d_rows[m] || !d_outputs[m]) return mhcudaInvalidArguments;
+    d.weights = d_weights[m];
+    d.cols = d_cols[m];
+    d.indptr = d_rows[m];
+    d.out = d_outputs[m];
+    d.rows = lengths[m];
+    plan_threads += static_cast<uint64_t>(lengths[m]) + 1;
+  }
+  if (plan_threads >= 0xFFFFFFFFull) return mhcudaInvalidArguments;
+  if (plan_threads == 0) return mhcudaSuccess;  // no matrix has rows
+  std::lock_guard<std::mutex> lock(gen->mu);
+  MHB_ON_DEVICE(gen);
+  const cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : gen->stream;
+
+  // Kernel variant as for one large launch; the chunk size is chosen on the
+  // device from the batch's nnz (batch_setup_kernel).
+  const HashPlan vp = make_plan(gen, 1ull << 30, 1ull << 20);
+  const int bps = mhb::hash_blocks_per_sm(vp.spl, vp.minb, gen->s_pad);
+  const uint64_t resident_warps =
+      static_cast<uint64_t>(gen->sm_count) * bps * (mhb::kHashBlock / 32);
+  TuneChoice tc{};
+  const int waves = std::max(1, env_int("MHCUDA_B200_WAVES", static_cast<int>(tc.waves)));
+  const uint64_t max_chunks64 = count + resident_warps * 8 + 1;
+  if (max_chunks64 >= 0xFFFFFFFFull) return mhcudaInvalidArguments;
+  const uint32_t max_chunks = static_cast<uint32_t>(max_chunks64);
+  HashPlan big{};
+  big.nchunks = max_chunks;
+  HashArgs base{};
+  MHCUDAResult r = prepare_launch(gen, 0, 0, big, &base);
+  if (r != mhcudaSuccess) return r;
+  MHB_CHECK(gen, gen->d_chunk_owner.ensure(static_cast<size_t>(max_chunks) * 4),
+            mhcudaMemoryAllocationFailure);
+  MHB_CHECK(gen, gen->d_batch_plan.ensure(sizeof(mhb::BatchPlan)), mhcudaMemoryAllocationFailure);
+  base.ntiles = vp.ntiles;
+
+  // The batch's entry: descriptors on the device (uploaded once) and, from
+  // its second call on, a CUDA graph of the launches.
+  const size_t mats_bytes = static_cast<size_t>(count) * sizeof(mhb::BatchMatrix);
+  const size_t desc_bytes = ((mats_bytes + 255) & ~static_cast<size_t>(255)) +
+                            static_cast<size_t>(count) * sizeof(uint32_t);
+  const void *batch_scratch[2] = {gen->d_chunk_owner.ptr, gen->d_batch_plan.ptr};
+  std::vector<unsigned char> key(mats_bytes + count * sizeof(uint32_t) + sizeof(st) +
+                                 sizeof(base) + sizeof(vp) + sizeof(batch_scratch));
+  {
+    unsigned char *k = key.data();
+    memcpy(k, mats.data(), mats_bytes);
+    k += mats_bytes;
+    memcpy(k, plan_base.data(), count * sizeof(uint32_t));
+    k += count * sizeof(uint32_t);
+    memcpy(k, &st, sizeof(st));
+    k += sizeof(st);
+    memcpy(k, &base, sizeof(base));
+    k += sizeof(base);
+    memcpy(k, &vp, sizeof(vp));
+    k += sizeof(vp);
+    memcpy(k, batch_scratch, sizeof(batch_scratch));
+  }
+  BatchEntry *e = nullptr;
+  for (auto &x : gen->batches)
+    if (x->key == key) e = x.get();
+  if (!e) {
+    constexpr size_t kMaxBatches = 8;
+    if (gen->batches.size() == kMaxBatches) gen->batches.erase(gen->batches.begin());
+    std::unique_ptr<BatchEntry> ne(new BatchEntry());
+    ne->key = std::move(key);
+    MHB_CHECK(gen, cudaEventCreateWithFlags(&ne->used, cudaEventDisableTiming), mhcudaRuntimeError);
+    MHB_CHECK(gen, ne->desc.ensure(desc_bytes), mhcudaMemoryAllocationFailure);
+    MHB_CHECK(gen, ne->staging.ensure(desc_bytes), mhcudaMemoryAllocationFailure);
+    unsigned char *h = ne->staging.as<unsigned char>();
+    memcpy(h, mats.data(), mats_bytes);
+    memcpy(h + desc_bytes - count * sizeof(uint32_t), plan_base.data(), count * sizeof(uint32_t));
+    MHB_CHECK(gen, cudaMemcpyAsync(ne->desc.ptr, h, desc_bytes, cudaMemcpyHostToDevice, st),
+              mhcudaMemoryCopyError);
+    gen->batches.push_back(std::move(ne));
+    e = gen->batches.back().get();
+  }
+  mhb::BatchArgs b{};
+  b.base = base;
+  b.mats = e->desc.as<mhb::BatchMatrix>();
+  b.plan_base = reinterpret_cast<const uint32_t *>(e->desc.as<unsigned char>() + desc_bytes -
+                                                   count * sizeof(uint32_t));
+  b.count = count;
+  b.max_chunks = max_chunks;
+  b.plan = gen->d_batch_plan.as<mhb::BatchPlan>();
+  b.chunk_owner = gen->d_chunk_owner.as<uint32_t>();
+  b.target_items = resident_warps * static_cast<uint64_t>(waves);
+  b.want_items = resident_warps * 8;
+  HashPlan lp = vp;
+  lp.grid = static_cast<uint32_t>(static_cast<uint64_t>(gen->sm_count) * bps);
+  const uint32_t pt = static_cast<uint32_t>(plan_threads);
+  auto enqueue = [&]() -> MHCUDAResult {
+    MHB_CHECK(gen, cudaMemsetAsync(base.status, 0, sizeof(uint32_t), st), mhcudaRuntimeError);
+    MHB_CHECK(gen, mhb::launch_batch(b, lp, pt, st), mhcudaRuntimeError);
+    return mhcudaSuccess;
+  };
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  MHB_CHECK(gen, cudaStreamIsCapturing(st, &cap), mhcudaRuntimeError);
+  const bool graphs = !gen->profiling && cap == cudaStreamCaptureStatusNone &&
+                      env_int("MHCUDA_B200_NO_GRAPHS", 0) == 0;
+  if (graphs && !e->exec && e->seen >= 1) {
+    cudaGraph_t graph = nullptr;
+    MHB_CHECK(gen, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), mhcudaRuntimeError);
+    r = enqueue();
+    const cudaError_t end = cudaStreamEndCapture(st, &graph);
+    if (r != mhcudaSuccess || end != cudaSuccess) {
+      cudaGetLastError();
+      if (graph) cudaGraphDestroy(graph);
+      return r != mhcudaSuccess ? r : mhcudaRuntimeError;
+    }
+    const cudaError_t inst = cudaGraphInstantiate(&e->exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (inst != cudaSuccess) {
+      e->exec = nullptr;
+      MHB_CHECK(gen, inst, mhcudaRuntimeError);
+    }
+  }
+  std::pair<cudaEvent_t, cudaEvent_t> *ev = nullptr;
+  if (gen->profiling) {
+    if (gen->prof_used == gen->prof_events.size()) {
+      std::pair<cudaEvent_t, cudaEvent_t> pe{nullptr, nullptr};
+      MHB_CHECK(gen, cudaEventCreate(&pe.first), mhcudaRuntimeError);
+      MHB_CHECK(gen, cudaEventCreate(&pe.second), mhcudaRuntimeError);
+      gen->prof_events.push_back(pe);
+    }
+    ev = &gen->prof_events[gen->prof_used++];
+    MHB_CHECK(gen, cudaEventRecord(ev->first, st), mhcudaRuntimeError);
+  }
+  if (graphs && e->exec) {
+    MHB_CHECK(gen, cudaGraphLaunch(e->exec, st), mhcudaRuntimeError);
+  } else {
+    r = enqueue();
+    if (r != mhcudaSuccess) return r;
+  }
+  if (ev) MHB_CHECK(gen, cudaEventRecord(ev->second, st), mhcudaRuntimeError);
+  ++e->seen;
+  if (cap == cudaStreamCaptureStatusNone)
+    MHB_CHECK(gen, cudaEventRecord(e->used, st), mhcudaRuntimeError);
+  return mhcudaSuccess;
+}
+
 enum MHCUDAResult mhcuda_autotune(const MinhashCudaGenerator *gen, const float *d_weights,
                                   const uint32_t *d_cols, const uint32_t *d_rows, uint32_t length,
                                   uint32_t nnz, uint32_t *d_output, void *stream,
@@ -1083,7 +1343,7 @@ enum MHCUDAResult mhcuda_autotune(const MinhashCudaGenerator *gen, const float *
   if (!gen || !d_rows || !d_output || length == 0 || (nnz && (!d_weights || !d_cols)))
     return mhcudaInvalidArguments;
   std::lock_guard<std::mutex> lock(gen->mu);
-  MHB_CHECK(gen, cudaSetDevice(gen->device), mhcudaNoSuchDevice);
+  MHB_ON_DEVICE(gen);
   const cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : gen->stream;
   // Candidates: samples per lane (lane utilisation of the last tile >= 1/2),
   // register budget of the 4-sample variant, and chunk granularity.
@@ -1142,7 +1402,7 @@ enum MHCUDAResult mhcuda_autotune(const MinhashCudaGenerator *gen, const float *
 enum MHCUDAResult mhcuda_device_status(const MinhashCudaGenerator *gen) {
   if (!gen) return mhcudaInvalidArguments;
   std::lock_guard<std::mutex> lock(gen->mu);
-  MHB_CHECK(gen, cudaSetDevice(gen->device), mhcudaNoSuchDevice);
+  MHB_ON_DEVICE(gen);
   MHB_CHECK(gen, cudaDeviceSynchronize(), mhcudaRuntimeError);
   if (!gen->d_status.ptr) return mhcudaSuccess;
   const MHCUDAResult r = read_status(gen, gen->stream);
@@ -1156,7 +1416,7 @@ enum MHCUDAResult mhcuda_calc_batch(const MinhashCudaGenerator *gen, uint32_t co
                                     uint32_t *const *outputs) {
   if (!gen || !weights || !cols || !rows || !lengths || !outputs) return mhcudaInvalidArguments;
   std::lock_guard<std::mutex> lock(gen->mu);
-  MHB_CHECK(gen, cudaSetDevice(gen->device), mhcudaNoSuchDevice);
+  MHB_ON_DEVICE(gen);
   // Per-matrix nnz; validated before any device work.
   std::vector<uint64_t> nnz_of(count, 0);
   for (uint32_t i = 0; i < count; ++i) {
@@ -1374,10 +1634,9 @@ enum MHCUDAResult mhcuda_debug_device_logf(uint32_t devices, const float *in, fl
                                            uint64_t n) {
   if (!in || !out) return mhcudaInvalidArguments;
   const int dev = pick_device(devices);
-  if (dev < 0 || cudaSetDevice(dev) != cudaSuccess) {
-    cudaGetLastError();
-    return mhcudaNoSuchDevice;
-  }
+  if (dev < 0) return mhcudaNoSuchDevice;
+  mhb::DeviceGuard on_device(dev);
+  if (!on_device.ok()) return mhcudaNoSuchDevice;
   if (n == 0) return mhcudaSuccess;
   DevBuf a, b;
   if (a.ensure(n * 4) != cudaSuccess || b.ensure(n * 4) != cudaSuccess)
@@ -1403,7 +1662,7 @@ enum MHCUDAResult mhcuda_profile_read(const MinhashCudaGenerator *gen, double *h
                                       uint64_t *launches) {
   if (!gen || !hash_ms || !launches) return mhcudaInvalidArguments;
   std::lock_guard<std::mutex> lock(gen->mu);
-  MHB_CHECK(gen, cudaSetDevice(gen->device), mhcudaNoSuchDevice);
+  MHB_ON_DEVICE(gen);
   double total = 0.0;
   for (size_t i = 0; i < gen->prof_used; ++i) {
     MHB_CHECK(gen, cudaEventSynchronize(gen->prof_events[i].second), mhcudaRuntimeError);

@@ -30,6 +30,7 @@
 //  - work is cut by nnz, not by rows, so one 50k-nnz row and many 5-nnz rows
 //    cost the same per item; rows that cross a chunk boundary are merged by
 //    a finalize pass (tie -> earlier position, as the strict '<' scan).
+#include <algorithm>
 #include <cfloat>
 #include <cstdint>
 
@@ -38,10 +39,44 @@
 namespace mhb {
 namespace {
 
+#ifndef MHB_L2_HINTS
+#define MHB_L2_HINTS 0
+#endif
+#ifndef MHB_FLOOR_RM
+#define MHB_FLOOR_RM 0
+#endif
+#ifndef MHB_SPAD_TEMPLATES
+#define MHB_SPAD_TEMPLATES 0
+#endif
+
+__device__ __forceinline__ uint64_t l2_policy_evict_first() {
+  uint64_t pol;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+__device__ __forceinline__ uint64_t l2_policy_evict_last() {
+  uint64_t pol;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+
 template <int SPL>
 struct Lanes {
   float v[SPL];
-  __device__ __forceinline__ void load(const float *__restrict__ p) {
+  __device__ __forceinline__ void load(const float *__restrict__ p, uint64_t pol) {
+#if MHB_L2_HINTS & 2
+    if constexpr (SPL == 4) {
+      asm("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+          : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]) : "l"(p), "l"(pol));
+    } else if constexpr (SPL == 2) {
+      asm("ld.global.nc.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;"
+          : "=f"(v[0]), "=f"(v[1]) : "l"(p), "l"(pol));
+    } else {
+      asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v[0]) : "l"(p), "l"(pol));
+    }
+    return;
+#endif
+    (void)pol;
     if constexpr (SPL == 4) {
       const float4 x = __ldg(reinterpret_cast<const float4 *>(p));
       v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
@@ -100,8 +135,10 @@ __device__ __forceinline__ void wmh_update(float t, float r, float c, float b, u
 // only decides t when it equals the exact one), so tracking the position
 // instead of (k, t) changes nothing but the work per evaluation.
 // (uint32)(int32)t as kernel.cu:108; the GPU conversion saturates.
+// A position outside [0, nnz) (none found, or a partial that a failed launch
+// left unwritten) yields kNone and reads nothing.
 __device__ __forceinline__ uint2 resolve(const HashArgs &a, uint32_t pos, uint32_t s) {
-  if (pos == kNone) return make_uint2(kNone, kNone);
+  if (pos >= a.nnz) return make_uint2(kNone, kNone);
   const uint32_t k = a.cols[pos];
   // An invalid column was evaluated as column 0 and failed the call: keep
   // the parameter reads in bounds.
@@ -112,10 +149,10 @@ __device__ __forceinline__ uint2 resolve(const HashArgs &a, uint32_t pos, uint32
   return make_uint2(k, static_cast<uint32_t>(static_cast<int32_t>(t)));
 }
 
-// chunk_row[c] = first row whose first position is >= c*chunk (rows if none).
-__global__ void plan_kernel(const HashArgs a) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i > a.rows) return;
+// chunk_row[c] = first row whose first position is >= c*chunk (rows if none),
+// for the chunks whose first owned row is row i (i == rows: the chunks past
+// the last row start); also validates the offsets.
+__device__ __forceinline__ void plan_row(const HashArgs &a, uint32_t i) {
   const uint32_t base = a.indptr[0];
   uint32_t start, c_hi;
   if (i < a.rows) {
@@ -138,6 +175,11 @@ __global__ void plan_kernel(const HashArgs a) {
   (void)start;
 }
 
+__global__ void plan_kernel(const HashArgs a) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i <= a.rows) plan_row(a, i);
+}
+
 template <int SPL>
 struct RowState {
   float mn[SPL];
@@ -157,7 +199,11 @@ __device__ __forceinline__ void store_final(const HashArgs &a, uint32_t row, uin
   uint32_t *o = a.out + (static_cast<size_t>(row) * a.samples + s0) * 2;
 #pragma unroll
   for (int j = 0; j < SPL; ++j) {
+#if MHB_L2_HINTS & 4
+    if (s0 + j < a.samples) __stcs(reinterpret_cast<uint2 *>(o + 2 * j), resolve(a, st.pos[j], s0 + j));
+#else
     if (s0 + j < a.samples) *reinterpret_cast<uint2 *>(o + 2 * j) = resolve(a, st.pos[j], s0 + j);
+#endif
   }
 }
 
@@ -223,11 +269,20 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, uint32_t 
 // addresses 16-byte aligned, bytes a multiple of 16.  No multicast.
 __device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, uint32_t bytes,
                                               unsigned long long *bar) {
+#if MHB_L2_HINTS & 1
+  // The CSR is read once per launch: evict it from L2 before the parameters.
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
+      " [%0], [%1], %2, [%3], %4;" ::"r"(smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar)), "l"(l2_policy_evict_first())
+      : "memory");
+#else
   asm volatile(
       "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
           smem_addr(dst)),
       "l"(src), "r"(bytes), "r"(smem_addr(bar))
       : "memory");
+#endif
 }
 
 // Lane 0 starts the copy of positions [ws, ws + n) into buffer `b`: the
@@ -296,10 +351,11 @@ __device__ __forceinline__ bool finish_window(const HashArgs &a, WarpStage &st, 
 template <int SPL>
 struct Params {
   Lanes<SPL> r, c, b;
-  __device__ __forceinline__ void load(const float *__restrict__ col_base, uint32_t s_pad) {
-    r.load(col_base);
-    c.load(col_base + s_pad);
-    b.load(col_base + 2 * s_pad);
+  __device__ __forceinline__ void load(const float *__restrict__ col_base, uint32_t s_pad,
+                                       uint64_t pol) {
+    r.load(col_base, pol);
+    c.load(col_base + s_pad, pol);
+    b.load(col_base + 2 * s_pad, pol);
   }
 };
 
@@ -368,12 +424,25 @@ __device__ __forceinline__ void eval_all(const Params<SPL> &p, float w, uint32_t
       asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y1) : "f"(p.r.v[j + 1]));
       const F2 qa = mul2(ww, f2(y0, y1));
       const F2 va = add2(qa, f2(p.b.v[j], p.b.v[j + 1]));
-      float v0, v1, q0, q1;
-      split(va, v0, v1);
+      float q0, q1;
       split(qa, q0, q1);
+#if MHB_FLOOR_RM
+      // floor(v) = RM(v + 1.5*2^23) - 1.5*2^23 for |v| < 2^22 (the sum lies in
+      // [2^23, 2^24), where rounding toward -inf to an integer is floor); for
+      // larger |v| the margin m >= 16 leaves t undecided.
+      const F2 magic{0x4B4000004B400000ull};  // (1.5*2^23, 1.5*2^23)
+      F2 tt;
+      asm("add.rm.f32x2 %0, %1, %2;" : "=l"(tt.v) : "l"(va.v), "l"(magic.v));
+      tt = sub2(tt, magic);
+      split(tt, t[j], t[j + 1]);
+      const F2 fr = sub2(va, tt);
+#else
+      float v0, v1;
+      split(va, v0, v1);
       t[j] = floorf(v0);
       t[j + 1] = floorf(v1);
       const F2 fr = sub2(va, f2(t[j], t[j + 1]));
+#endif
       const F2 s = f2(__fadd_rn(fabsf(q0), fabsf(p.b.v[j])),
                       __fadd_rn(fabsf(q1), fabsf(p.b.v[j + 1])));
       const F2 lim = fma2(s, f2(-kTMargin, -kTMargin), f2(0.5f - kTMargin, 0.5f - kTMargin));
@@ -410,34 +479,55 @@ __device__ __forceinline__ void eval_all(const Params<SPL> &p, float w, uint32_t
   }
 }
 
-template <int SPL, int MINB>
-__global__ void __launch_bounds__(kHashBlock, MINB) hash_kernel(const HashArgs a) {
-  __shared__ WarpStage stage_all[kHashBlock / 32];
-  if (*a.status & kStatusBadIndptr) return;
-  const uint32_t lane = threadIdx.x & 31u;
-  WarpStage &stg = stage_all[threadIdx.x >> 5];
-  if (lane == 0) {
-    mbar_init(&stg.bar[0], 1);
-    mbar_init(&stg.bar[1], 1);
+// Per-warp state of the hash kernels: the staging buffers, their barrier
+// phases and the launch-wide constants of the item loop.
+struct WarpCtx {
+  WarpStage *stg;
+  uint32_t parity;  // bit b: phase parity to wait for on buffer b
+  uint32_t lane;
+  uint64_t pol;     // L2 policy of the parameter loads
+};
+
+__device__ __forceinline__ void warp_ctx_init(WarpCtx &w, WarpStage *stage_all) {
+  w.lane = threadIdx.x & 31u;
+  w.stg = &stage_all[threadIdx.x >> 5];
+  if (w.lane == 0) {
+    mbar_init(&w.stg->bar[0], 1);
+    mbar_init(&w.stg->bar[1], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncwarp();
-  uint32_t parity = 0;  // bit b: phase parity to wait for on buffer b
+  w.parity = 0;
+#if MHB_L2_HINTS & 2
+  w.pol = l2_policy_evict_last();
+#else
+  w.pol = 0;
+#endif
+}
 
-  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+// One (chunk c, sample tile) item over the CSR of `a`: finishes the rows
+// that lie inside chunk c and leaves partial minima for the rows that cross
+// its ends.  Returns false after an error exit (status flagged, in-flight
+// staging copies drained); the warp must then stop.
+// SPAD: the generator's s_pad when it is known at compile time (0: read it
+// from the arguments), which turns the parameter-block addressing into one
+// wide multiply-add and immediate load offsets.
+template <int SPL, int SPAD>
+__device__ __forceinline__ bool hash_item(const HashArgs &a, uint32_t c, uint32_t tile,
+                                          WarpCtx &wc) {
+  const uint32_t lane = wc.lane;
+  WarpStage &stg = *wc.stg;
+  uint32_t &parity = wc.parity;
+  const uint64_t pol = wc.pol;
   const uint32_t base = a.indptr[0];
-  const uint32_t items = a.nchunks * a.ntiles;
-  const size_t col_stride = static_cast<size_t>(3) * a.s_pad;
+  const uint32_t spad = SPAD ? static_cast<uint32_t>(SPAD) : a.s_pad;
+  const size_t col_stride = static_cast<size_t>(3) * (SPAD ? static_cast<uint32_t>(SPAD) : a.s_pad);
   // Bulk copies only from device memory; mapped host CSR is read by the lanes.
   const bool bulk_ok = !a.host_csr && ((reinterpret_cast<uintptr_t>(a.weights) |
                                         reinterpret_cast<uintptr_t>(a.cols)) & 15u) == 0;
-
-  for (uint32_t item = gw; item < items; item += nw) {
-    const uint32_t c = item / a.ntiles;
-    const uint32_t tile = item - c * a.ntiles;
+  {
     const uint32_t s0 = tile * (32u * SPL) + lane * SPL;
-    const bool active = s0 < a.s_pad;
+    const bool active = s0 < spad;
     // Lanes past the last sample read the tile's first samples (in bounds)
     // and never store, so parameter loads need no branch.
     const float *__restrict__ pbase = a.params + (active ? s0 : tile * (32u * SPL));
@@ -494,7 +584,7 @@ __global__ void __launch_bounds__(kHashBlock, MINB) hash_kernel(const HashArgs a
       if (!finish_window(a, stg, b, (parity >> b) & 1u, ws, n, bulk_ok, lane)) {
         if (lane == 0) atomicOr(a.status, kStatusStall);
         drain(k);
-        return;
+        return false;
       }
       parity ^= 1u << b;
       const float *__restrict__ lw = stg.w[b];
@@ -504,7 +594,7 @@ __global__ void __launch_bounds__(kHashBlock, MINB) hash_kernel(const HashArgs a
       // (finish_window).
       Params<SPL> A, B;
       uint32_t dA = cl[0], dB = 0;
-      A.load(pbase + dA * col_stride, a.s_pad);
+      A.load(pbase + dA * col_stride, spad, pol);
       uint32_t i = 0;
       while (i < n) {
         // Row boundaries (warp-uniform): finish rows, start the next owned one.
@@ -513,7 +603,7 @@ __global__ void __launch_bounds__(kHashBlock, MINB) hash_kernel(const HashArgs a
           if (r_next >= r_stop) {  // only reachable with inconsistent offsets
             if (lane == 0) atomicOr(a.status, kStatusBadIndptr);
             drain(k + 1);
-            return;
+            return false;
           }
           row = r_next++;
           row_end = a.indptr[row + 1] - base;
@@ -525,16 +615,16 @@ __global__ void __launch_bounds__(kHashBlock, MINB) hash_kernel(const HashArgs a
         // evaluated, A for i+2 while B is evaluated.
         while (i + 1 < seg) {  // i + 2 <= n
           dB = cl[i + 1];
-          B.load(pbase + dB * col_stride, a.s_pad);
+          B.load(pbase + dB * col_stride, spad, pol);
           eval_all<SPL>(A, lw[i], ws + i, active, st);
           dA = cl[i + 2];
-          A.load(pbase + dA * col_stride, a.s_pad);
+          A.load(pbase + dA * col_stride, spad, pol);
           eval_all<SPL>(B, lw[i + 1], ws + i + 1, active, st);
           i += 2;
         }
         if (i < seg) {  // i + 1 <= n
           dB = cl[i + 1];
-          B.load(pbase + dB * col_stride, a.s_pad);
+          B.load(pbase + dB * col_stride, spad, pol);
           eval_all<SPL>(A, lw[i], ws + i, active, st);
           ++i;
           A = B;
@@ -557,6 +647,22 @@ __global__ void __launch_bounds__(kHashBlock, MINB) hash_kernel(const HashArgs a
       flush();
     }
   }
+  return true;
+}
+
+template <int SPL, int MINB, int SPAD>
+__global__ void __launch_bounds__(kHashBlock, MINB) hash_kernel(const HashArgs a) {
+  __shared__ WarpStage stage_all[kHashBlock / 32];
+  if (*a.status & kStatusBadIndptr) return;
+  WarpCtx wc;
+  warp_ctx_init(wc, stage_all);
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t items = a.nchunks * a.ntiles;
+  for (uint32_t item = gw; item < items; item += nw) {
+    const uint32_t c = item / a.ntiles;
+    if (!hash_item<SPL, SPAD>(a, c, item - c * a.ntiles, wc)) return;
+  }
 }
 
 // Merge the partials of every row that leaves its own chunk: one warp per
@@ -567,56 +673,260 @@ __global__ void __launch_bounds__(kHashBlock, MINB) hash_kernel(const HashArgs a
 // ties, as the scan of kernel.cu:106 does.
 constexpr uint32_t kFinalizeUnroll = 8;
 
+// Merges, for sample s, the partials of the row that leaves chunk c (if one
+// does) and writes its output pair.
+__device__ __forceinline__ void finalize_item(const HashArgs &a, uint32_t c, uint32_t s) {
+  const uint32_t base = a.indptr[0];
+  const uint32_t r0 = a.chunk_row[c];
+  const uint32_t r1 = (c + 1 < a.nchunks) ? a.chunk_row[c + 1] : a.rows;
+  if (r1 <= r0) return;
+  const uint32_t row = r1 - 1;
+  const uint32_t end = a.indptr[row + 1] - base;
+  const uint32_t ce = c * a.chunk + min(a.chunk, a.nnz - c * a.chunk);
+  if (end <= ce || s >= a.samples) return;
+  const uint32_t c_last = (end - 1) / a.chunk;
+  const size_t stride = 2 * static_cast<size_t>(a.s_pad);  // one chunk's two slots
+  size_t off = static_cast<size_t>(2 * c + 1) * a.s_pad + s;
+  float mn = a.part_ln[off];
+  uint32_t kp = a.part_kt[off].x;
+  off = static_cast<size_t>(2 * (c + 1)) * a.s_pad + s;
+  uint32_t cc = c + 1;
+  for (; cc + kFinalizeUnroll - 1 <= c_last; cc += kFinalizeUnroll) {
+    float m[kFinalizeUnroll];
+    uint32_t k[kFinalizeUnroll];
+#pragma unroll
+    for (uint32_t u = 0; u < kFinalizeUnroll; ++u) {
+      m[u] = a.part_ln[off + u * stride];
+      k[u] = a.part_kt[off + u * stride].x;
+    }
+#pragma unroll
+    for (uint32_t u = 0; u < kFinalizeUnroll; ++u) {
+      const bool lt = m[u] < mn;
+      mn = lt ? m[u] : mn;
+      kp = lt ? k[u] : kp;
+    }
+    off += kFinalizeUnroll * stride;
+  }
+  for (; cc <= c_last; ++cc, off += stride) {
+    const float m2 = a.part_ln[off];
+    const uint32_t k2 = a.part_kt[off].x;
+    const bool lt = m2 < mn;
+    mn = lt ? m2 : mn;
+    kp = lt ? k2 : kp;
+  }
+  uint32_t *o = a.out + (static_cast<size_t>(row) * a.samples + s) * 2;
+  *reinterpret_cast<uint2 *>(o) = resolve(a, kp, s);
+}
+
 __global__ void finalize_kernel(const HashArgs a) {
-  if (*a.status & kStatusBadIndptr) return;
+  // Any failure (invalid CSR, a staging copy that gave up) fails the call;
+  // the partials a failed hash launch left may be stale, so none is merged.
+  if (*a.status != 0) return;
   const uint32_t lane = threadIdx.x & 31u;
   const uint64_t gw = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) >> 5;
   const uint64_t nw = (gridDim.x * static_cast<uint64_t>(blockDim.x)) >> 5;
-  const uint32_t base = a.indptr[0];
   const uint32_t stiles = (a.samples + 31) / 32;
   const uint64_t items = static_cast<uint64_t>(a.nchunks) * stiles;
-  const size_t stride = 2 * static_cast<size_t>(a.s_pad);  // one chunk's two slots
   for (uint64_t it = gw; it < items; it += nw) {
     const uint32_t c = static_cast<uint32_t>(it / stiles);
     const uint32_t s = static_cast<uint32_t>(it - static_cast<uint64_t>(c) * stiles) * 32 + lane;
-    const uint32_t r0 = a.chunk_row[c];
-    const uint32_t r1 = (c + 1 < a.nchunks) ? a.chunk_row[c + 1] : a.rows;
-    if (r1 <= r0) continue;
-    const uint32_t row = r1 - 1;
-    const uint32_t end = a.indptr[row + 1] - base;
-    const uint32_t ce = c * a.chunk + min(a.chunk, a.nnz - c * a.chunk);
-    if (end <= ce || s >= a.samples) continue;
-    const uint32_t c_last = (end - 1) / a.chunk;
-    size_t off = static_cast<size_t>(2 * c + 1) * a.s_pad + s;
-    float mn = a.part_ln[off];
-    uint32_t kp = a.part_kt[off].x;
-    off = static_cast<size_t>(2 * (c + 1)) * a.s_pad + s;
-    uint32_t cc = c + 1;
-    for (; cc + kFinalizeUnroll - 1 <= c_last; cc += kFinalizeUnroll) {
-      float m[kFinalizeUnroll];
-      uint32_t k[kFinalizeUnroll];
-#pragma unroll
-      for (uint32_t u = 0; u < kFinalizeUnroll; ++u) {
-        m[u] = a.part_ln[off + u * stride];
-        k[u] = a.part_kt[off + u * stride].x;
-      }
-#pragma unroll
-      for (uint32_t u = 0; u < kFinalizeUnroll; ++u) {
-        const bool lt = m[u] < mn;
-        mn = lt ? m[u] : mn;
-        kp = lt ? k[u] : kp;
-      }
-      off += kFinalizeUnroll * stride;
+    finalize_item(a, c, s);
+  }
+}
+
+// ---- Device-resident batches ----------------------------------------------
+// Many CSR matrices hashed against one generator by one persistent launch.
+// Every matrix is cut into chunks of the same size; the batch's chunks are
+// numbered matrix after matrix, and a warp item is (batch chunk, sample
+// tile).  chunk_owner maps a batch chunk to its matrix, whose CSR, output and
+// slice of the chunk table and partials the item then works on exactly as a
+// single-matrix launch would: results equal one launch per matrix bit for bit
+// (a row's arg-min and its ties do not depend on how positions are cut).
+
+// HashArgs of matrix m inside batch b.
+__device__ __forceinline__ HashArgs matrix_view(const BatchArgs &b, const BatchMatrix &m,
+                                                uint32_t chunk) {
+  HashArgs v = b.base;
+  v.weights = m.weights;
+  v.cols = m.cols;
+  v.indptr = m.indptr;
+  v.out = m.out;
+  v.rows = m.rows;
+  v.nnz = m.nnz;
+  v.chunk = chunk;
+  v.nchunks = m.nchunks;
+  v.chunk_row = b.base.chunk_row + m.chunk_base;
+  v.part_ln = b.base.part_ln + static_cast<size_t>(2) * m.chunk_base * b.base.s_pad;
+  v.part_kt = b.base.part_kt + static_cast<size_t>(2) * m.chunk_base * b.base.s_pad;
+  return v;
+}
+
+constexpr int kSetupThreads = 1024;
+
+// Exclusive prefix sum over the block of one value per thread; returns this
+// thread's offset and writes the total to *total.
+__device__ __forceinline__ uint64_t block_exclusive_scan(uint64_t x, uint64_t *total) {
+  __shared__ uint64_t warp_sums[kSetupThreads / 32];
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  uint64_t incl = x;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint64_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+    if (lane >= static_cast<uint32_t>(o)) incl += y;
+  }
+  if (lane == 31) warp_sums[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    uint64_t w = lane < kSetupThreads / 32 ? warp_sums[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint64_t y = __shfl_up_sync(0xFFFFFFFFu, w, o);
+      if (lane >= static_cast<uint32_t>(o)) w += y;
     }
-    for (; cc <= c_last; ++cc, off += stride) {
-      const float m2 = a.part_ln[off];
-      const uint32_t k2 = a.part_kt[off].x;
-      const bool lt = m2 < mn;
-      mn = lt ? m2 : mn;
-      kp = lt ? k2 : kp;
+    warp_sums[lane] = w;  // inclusive over warps
+  }
+  __syncthreads();
+  const uint64_t before_warp = warp ? warp_sums[warp - 1] : 0;
+  *total = warp_sums[kSetupThreads / 32 - 1];
+  __syncthreads();
+  return before_warp + incl - x;
+}
+
+// One block of kSetupThreads: per-matrix nnz (validating the end offsets),
+// the batch's chunk size (the planner's rule applied to the whole batch, and
+// large enough that the chunks fit max_chunks), each matrix's chunk range
+// and the chunk -> matrix table.
+__global__ void __launch_bounds__(kSetupThreads) batch_setup_kernel(const BatchArgs b) {
+  const uint32_t t = threadIdx.x;
+  const uint32_t per = (b.count + kSetupThreads - 1) / kSetupThreads;
+  const uint32_t m0 = min(b.count, t * per), m1 = min(b.count, m0 + per);
+  uint64_t nnz_sum = 0, rows_sum = 0, nonempty = 0;
+  for (uint32_t m = m0; m < m1; ++m) {
+    BatchMatrix &mt = b.mats[m];
+    uint32_t n = 0;
+    if (mt.rows) {
+      const uint32_t s0 = mt.indptr[0], e = mt.indptr[mt.rows];
+      if (e < s0) {
+        atomicOr(b.base.status, kStatusBadIndptr);
+      } else {
+        n = e - s0;
+      }
+      ++nonempty;
     }
-    uint32_t *o = a.out + (static_cast<size_t>(row) * a.samples + s) * 2;
-    *reinterpret_cast<uint2 *>(o) = resolve(a, kp, s);
+    mt.nnz = n;
+    nnz_sum += n;
+    rows_sum += mt.rows;
+  }
+  uint64_t total_nnz, total_rows, total_nonempty;
+  block_exclusive_scan(nnz_sum, &total_nnz);
+  block_exclusive_scan(rows_sum, &total_rows);
+  block_exclusive_scan(nonempty, &total_nonempty);
+  __shared__ uint32_t s_chunk;
+  if (t == 0) {
+    const uint64_t ntiles = b.base.ntiles;
+    uint64_t chunk = (total_nnz * ntiles + b.target_items - 1) / b.target_items;
+    const uint64_t avg_row = total_rows ? (total_nnz + total_rows - 1) / total_rows : 1;
+    chunk = max(chunk, min(4 * avg_row, static_cast<uint64_t>(1024)));
+    chunk = min(chunk, max(static_cast<uint64_t>(64),
+                           (total_nnz * ntiles + b.want_items - 1) / b.want_items));
+    // sum over matrices of ceil(nnz_m / chunk) <= total_nnz / chunk + nonempty
+    const uint64_t avail = b.max_chunks > total_nonempty ? b.max_chunks - total_nonempty : 1;
+    chunk = max(chunk, (total_nnz + avail - 1) / avail);
+    chunk = max(static_cast<uint64_t>(64), (chunk + 31) & ~static_cast<uint64_t>(31));
+    if (chunk > (1u << 24)) {
+      chunk = 1u << 24;
+      if (total_nnz / chunk + total_nonempty > b.max_chunks) atomicOr(b.base.status, kStatusBadIndptr);
+    }
+    s_chunk = static_cast<uint32_t>(chunk);
+  }
+  __syncthreads();
+  const uint32_t chunk = s_chunk;
+  uint64_t my_chunks = 0;
+  for (uint32_t m = m0; m < m1; ++m) {
+    const BatchMatrix &mt = b.mats[m];
+    if (mt.rows) my_chunks += max(static_cast<uint64_t>(1), (static_cast<uint64_t>(mt.nnz) + chunk - 1) / chunk);
+  }
+  uint64_t total_chunks;
+  uint64_t cb = block_exclusive_scan(my_chunks, &total_chunks);
+  const bool fits = total_chunks <= b.max_chunks;
+  for (uint32_t m = m0; m < m1; ++m) {
+    BatchMatrix &mt = b.mats[m];
+    const uint32_t nc = mt.rows ? static_cast<uint32_t>(max(
+        static_cast<uint64_t>(1), (static_cast<uint64_t>(mt.nnz) + chunk - 1) / chunk)) : 0u;
+    mt.chunk_base = static_cast<uint32_t>(cb);
+    mt.nchunks = fits ? nc : 0u;
+    if (fits)
+      for (uint32_t c = 0; c < nc; ++c) b.chunk_owner[cb + c] = m;
+    cb += nc;
+  }
+  if (t == 0) {
+    if (!fits) atomicOr(b.base.status, kStatusBadIndptr);
+    b.plan->chunk = chunk;
+    b.plan->nchunks = fits ? static_cast<uint32_t>(total_chunks) : 0u;
+  }
+}
+
+// Matrix owning plan thread g: the last one whose plan_base is <= g (matrices
+// without rows own no threads and share the next matrix's plan_base).
+__device__ __forceinline__ uint32_t plan_owner(const BatchArgs &b, uint32_t g) {
+  uint32_t lo = 0, hi = b.count;  // answer in [lo, hi)
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (b.plan_base[mid] <= g) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void batch_plan_kernel(const BatchArgs b, uint32_t plan_threads) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= plan_threads || (*b.base.status & kStatusBadIndptr)) return;
+  const uint32_t m = plan_owner(b, g);
+  const BatchMatrix mt = b.mats[m];
+  if (!mt.rows || !mt.nchunks) return;
+  const HashArgs v = matrix_view(b, mt, b.plan->chunk);
+  plan_row(v, g - b.plan_base[m]);
+}
+
+// The matrix view of an item is kept in shared memory, one per warp: its
+// fields are read where the item needs them (per row or window), so the
+// evaluation loop's registers are the single-matrix kernel's.
+template <int SPL, int MINB, int SPAD>
+__global__ void __launch_bounds__(kHashBlock, MINB) hash_batch_kernel(const BatchArgs b) {
+  __shared__ WarpStage stage_all[kHashBlock / 32];
+  __shared__ HashArgs views[kHashBlock / 32];
+  if (*b.base.status & kStatusBadIndptr) return;
+  WarpCtx wc;
+  warp_ctx_init(wc, stage_all);
+  HashArgs &view = views[threadIdx.x >> 5];
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t ntiles = b.base.ntiles;
+  const uint32_t chunk = b.plan->chunk;
+  const uint32_t items = b.plan->nchunks * ntiles;
+  for (uint32_t item = gw; item < items; item += nw) {
+    const uint32_t gc = item / ntiles;
+    const uint32_t m = b.chunk_owner[gc];
+    const uint32_t base = b.mats[m].chunk_base;
+    __syncwarp();
+    if (wc.lane == 0) view = matrix_view(b, b.mats[m], chunk);
+    __syncwarp();
+    if (!hash_item<SPL, SPAD>(view, gc - base, item - gc * ntiles, wc)) return;
+  }
+}
+
+__global__ void finalize_batch_kernel(const BatchArgs b) {
+  if (*b.base.status != 0) return;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint64_t gw = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) >> 5;
+  const uint64_t nw = (gridDim.x * static_cast<uint64_t>(blockDim.x)) >> 5;
+  const uint32_t stiles = (b.base.samples + 31) / 32;
+  const uint32_t chunk = b.plan->chunk;
+  const uint64_t items = static_cast<uint64_t>(b.plan->nchunks) * stiles;
+  for (uint64_t it = gw; it < items; it += nw) {
+    const uint32_t gc = static_cast<uint32_t>(it / stiles);
+    const uint32_t s = static_cast<uint32_t>(it - static_cast<uint64_t>(gc) * stiles) * 32 + lane;
+    const BatchMatrix mt = b.mats[b.chunk_owner[gc]];
+    if (mt.nchunks < 2) continue;  // a matrix of one chunk has no partials to merge
+    const HashArgs v = matrix_view(b, mt, chunk);
+    finalize_item(v, gc - mt.chunk_base, s);
   }
 }
 
@@ -638,14 +948,50 @@ cudaError_t launch_plan(const HashArgs &a, cudaStream_t stream) {
 namespace {
 
 using HashFn = void (*)(const HashArgs);
+using BatchFn = void (*)(const BatchArgs);
 
-// Instantiated (samples per lane, minimum resident blocks per SM) variants.
-HashFn pick_hash(uint32_t spl, uint32_t minb) {
+BatchFn pick_batch(uint32_t spl, uint32_t minb, uint32_t s_pad) {
+#if MHB_SPAD_TEMPLATES
+  switch (spl * 100000 + minb * 10000 + s_pad) {
+    case 440128: return hash_batch_kernel<4, 4, 128>;
+    case 430128: return hash_batch_kernel<4, 3, 128>;
+    case 440256: return hash_batch_kernel<4, 4, 256>;
+    case 430256: return hash_batch_kernel<4, 3, 256>;
+    case 240064: return hash_batch_kernel<2, 4, 64>;
+    default: break;
+  }
+#else
+  (void)s_pad;
+#endif
   switch (spl * 10 + minb) {
-    case 44: return hash_kernel<4, 4>;
-    case 43: return hash_kernel<4, 3>;
-    case 24: return hash_kernel<2, 4>;
-    case 14: return hash_kernel<1, 4>;
+    case 44: return hash_batch_kernel<4, 4, 0>;
+    case 43: return hash_batch_kernel<4, 3, 0>;
+    case 24: return hash_batch_kernel<2, 4, 0>;
+    case 14: return hash_batch_kernel<1, 4, 0>;
+    default: return nullptr;
+  }
+}
+
+// Instantiated (samples per lane, minimum resident blocks per SM) variants,
+// with s_pad compiled in for the common sample counts.
+HashFn pick_hash(uint32_t spl, uint32_t minb, uint32_t s_pad) {
+#if MHB_SPAD_TEMPLATES
+  switch (spl * 100000 + minb * 10000 + s_pad) {
+    case 440128: return hash_kernel<4, 4, 128>;
+    case 430128: return hash_kernel<4, 3, 128>;
+    case 440256: return hash_kernel<4, 4, 256>;
+    case 430256: return hash_kernel<4, 3, 256>;
+    case 240064: return hash_kernel<2, 4, 64>;
+    default: break;
+  }
+#else
+  (void)s_pad;
+#endif
+  switch (spl * 10 + minb) {
+    case 44: return hash_kernel<4, 4, 0>;
+    case 43: return hash_kernel<4, 3, 0>;
+    case 24: return hash_kernel<2, 4, 0>;
+    case 14: return hash_kernel<1, 4, 0>;
     default: return nullptr;
   }
 }
@@ -653,7 +999,7 @@ HashFn pick_hash(uint32_t spl, uint32_t minb) {
 }  // namespace
 
 cudaError_t launch_hash(const HashArgs &a, const HashPlan &plan, cudaStream_t stream) {
-  const HashFn fn = pick_hash(plan.spl, plan.minb);
+  const HashFn fn = pick_hash(plan.spl, plan.minb, a.s_pad);
   if (!fn) return cudaErrorInvalidValue;
   fn<<<plan.grid, kHashBlock, 0, stream>>>(a);
   return cudaGetLastError();
@@ -668,8 +1014,23 @@ cudaError_t launch_finalize(const HashArgs &a, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
-int hash_blocks_per_sm(uint32_t spl, uint32_t minb) {
-  const HashFn fn = pick_hash(spl, minb);
+cudaError_t launch_batch(const BatchArgs &b, const HashPlan &plan, uint32_t plan_threads,
+                         cudaStream_t stream) {
+  const BatchFn fn = pick_batch(plan.spl, plan.minb, b.base.s_pad);
+  if (!fn || b.count == 0 || b.max_chunks == 0) return cudaErrorInvalidValue;
+  batch_setup_kernel<<<1, kSetupThreads, 0, stream>>>(b);
+  if (plan_threads)
+    batch_plan_kernel<<<(plan_threads + 255) / 256, 256, 0, stream>>>(b, plan_threads);
+  fn<<<plan.grid, kHashBlock, 0, stream>>>(b);
+  const uint64_t stiles = (b.base.samples + 31) / 32;
+  uint64_t blocks = (static_cast<uint64_t>(b.max_chunks) * stiles + 7) / 8;
+  blocks = std::min<uint64_t>(std::max<uint64_t>(blocks, 1), 8192);
+  finalize_batch_kernel<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(b);
+  return cudaGetLastError();
+}
+
+int hash_blocks_per_sm(uint32_t spl, uint32_t minb, uint32_t s_pad) {
+  const HashFn fn = pick_hash(spl, minb, s_pad);
   int n = 0;
   if (!fn || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kHashBlock, 0) != cudaSuccess) {
     cudaGetLastError();
@@ -678,8 +1039,8 @@ int hash_blocks_per_sm(uint32_t spl, uint32_t minb) {
   return n > 0 ? n : 1;
 }
 
-size_t hash_kernel_registers(uint32_t spl, uint32_t minb) {
-  const HashFn fn = pick_hash(spl, minb);
+size_t hash_kernel_registers(uint32_t spl, uint32_t minb, uint32_t s_pad) {
+  const HashFn fn = pick_hash(spl, minb, s_pad);
   cudaFuncAttributes attr{};
   if (!fn || cudaFuncGetAttributes(&attr, fn) != cudaSuccess) return 0;
   return attr.numRegs;

@@ -74,7 +74,8 @@ enum MHCUDAResult mhcuda_lsh_bands(const MinhashCudaGenerator *gen, const uint32
   if (!mhb::generator_view(gen, &g) || !d_hashes || !d_keys || band_width == 0 ||
       band_width > g.samples)
     return mhcudaInvalidArguments;
-  if (cudaSetDevice(g.device) != cudaSuccess) return mhcudaNoSuchDevice;
+  mhb::DeviceGuard on_device(g.device);
+  if (!on_device.ok()) return mhcudaNoSuchDevice;
   const uint32_t bands = g.samples / band_width;
   const uint64_t n = static_cast<uint64_t>(rows) * bands;
   if (n == 0) return mhcudaSuccess;
@@ -93,7 +94,8 @@ enum MHCUDAResult mhcuda_jaccard(const MinhashCudaGenerator *gen, const uint32_t
   mhb::GeneratorView g{};
   if (!mhb::generator_view(gen, &g) || !d_hashes || !d_pairs || !d_out)
     return mhcudaInvalidArguments;
-  if (cudaSetDevice(g.device) != cudaSuccess) return mhcudaNoSuchDevice;
+  mhb::DeviceGuard on_device(g.device);
+  if (!on_device.ok()) return mhcudaNoSuchDevice;
   if (npairs == 0) return mhcudaSuccess;
   const cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : g.stream;
   const uint64_t blocks = (npairs * 32 + 255) / 256;

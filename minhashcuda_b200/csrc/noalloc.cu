@@ -109,14 +109,12 @@ extern "C" enum MHCUDAResult mhcuda_calc_device_noalloc(
   if (end > kNoallocScratchBytes) return mhcudaInvalidArguments;
 
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (cudaSetDevice(g.device) != cudaSuccess) {
-    cudaGetLastError();
-    return mhcudaNoSuchDevice;
-  }
+  mhb::DeviceGuard on_device(g.device);
+  if (!on_device.ok()) return mhcudaNoSuchDevice;
   char *scratch = static_cast<char *>(noalloc_scratch_on(g.device));
   if (!scratch) return mhcudaRuntimeError;
   const cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : g.stream;
-  const int bps = mhb::hash_blocks_per_sm(plan.spl, plan.minb);
+  const int bps = mhb::hash_blocks_per_sm(plan.spl, plan.minb, s_pad);
   const uint64_t items = static_cast<uint64_t>(plan.nchunks) * plan.ntiles;
   const uint64_t want = (items + mhb::kHashBlock / 32 - 1) / (mhb::kHashBlock / 32);
   plan.grid = static_cast<uint32_t>(

@@ -201,7 +201,7 @@ MinhashCudaServer_::~MinhashCudaServer_() {
   work.notify_all();
   for (Lane &l : lanes)
     if (l.thread.joinable()) l.thread.join();
-  cudaSetDevice(device);
+  mhb::DeviceGuard on_device(device);
   for (Lane &l : lanes) {
     if (l.stream) cudaStreamSynchronize(l.stream);
     cudaFree(l.w);
@@ -283,7 +283,7 @@ MHCUDAResult MinhashCudaServer_::run_units(Lane &lane, const std::vector<Unit> &
   // even when rows are long (the plain plan keeps a few rows per chunk);
   // several lanes' launches overlap, so two are enough.
   mhb::HashPlan plan = mhb::plan_for_generator(units.front().req->gen, N, R, 2);
-  const int bps = mhb::hash_blocks_per_sm(plan.spl, plan.minb);
+  const int bps = mhb::hash_blocks_per_sm(plan.spl, plan.minb, s_pad);
   // Keep the chunk table and partials inside the lane's fixed scratch:
   // nchunks*4 <= unit, 2*nchunks*s_pad*4 <= 4*unit, 2*nchunks*s_pad*8 <= 8*unit.
   const uint64_t max_chunks = std::max<uint64_t>(
@@ -528,8 +528,12 @@ MinhashCudaServer *mhcuda_server_start(uint32_t devices, uint64_t hbm_budget_byt
   if (devices == 0) dev = 0;
   for (int d = 0; d < 32 && d < count && dev < 0; ++d)
     if (devices & (1u << d)) dev = d;
-  if (dev < 0 || cudaSetDevice(dev) != cudaSuccess) {
-    cudaGetLastError();
+  if (dev < 0) {
+    set(mhcudaNoSuchDevice);
+    return nullptr;
+  }
+  mhb::DeviceGuard on_device(dev);
+  if (!on_device.ok()) {
     set(mhcudaNoSuchDevice);
     return nullptr;
   }

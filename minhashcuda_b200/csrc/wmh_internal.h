@@ -69,14 +69,54 @@ struct HashArgs {
   uint32_t host_csr;         // weights/cols/indptr/out are mapped host memory
 };
 
+// One matrix of a device-resident batch (mhcuda_calc_batch_device).  The
+// host fills the CSR pointers, rows and plan_base; batch_setup_kernel fills
+// nnz, chunk_base and nchunks on the device.
+struct BatchMatrix {
+  const float *weights;    // weights[p] for relative position p
+  const uint32_t *cols;
+  const uint32_t *indptr;  // rows+1 absolute offsets, indptr[0] = offset of weights[0]
+  uint32_t *out;           // [rows][samples][2]
+  uint32_t rows;
+  uint32_t nnz;
+  uint32_t chunk_base;     // index of its first chunk in the batch's chunk space
+  uint32_t nchunks;        // 0 for a matrix without rows
+};
+
+// Work decomposition of a batch, computed on the device.
+struct BatchPlan {
+  uint32_t chunk;    // positions per chunk, the same for every matrix
+  uint32_t nchunks;  // chunks of all matrices
+};
+
+struct BatchArgs {
+  HashArgs base;          // generator fields, ntiles, status and the batch-wide scratch
+                          // (chunk_row, part_ln, part_kt indexed by batch chunk)
+  BatchMatrix *mats;      // [count]
+  const uint32_t *plan_base;  // [count] first plan thread of each matrix (rows+1 each)
+  uint32_t count;
+  uint32_t max_chunks;    // chunk slots the scratch holds
+  BatchPlan *plan;
+  uint32_t *chunk_owner;  // [max_chunks] matrix of each batch chunk
+  uint64_t target_items;  // warp items to aim for (resident warps x waves)
+  uint64_t want_items;    // items per launch below which chunks shrink (resident warps x 8)
+};
+
 // Launchers (hash_kernels.cu).  All enqueue on `stream` and return the launch
 // error, if any.
 cudaError_t launch_plan(const HashArgs &a, cudaStream_t stream);
 cudaError_t launch_hash(const HashArgs &a, const HashPlan &plan, cudaStream_t stream);
 cudaError_t launch_finalize(const HashArgs &a, cudaStream_t stream);
-// Blocks per SM the hash kernel reaches for a given samples-per-lane value.
-int hash_blocks_per_sm(uint32_t spl, uint32_t minb);
-size_t hash_kernel_registers(uint32_t spl, uint32_t minb);
+// A whole device-resident batch: setup (per-matrix nnz, chunk size, chunk
+// tables), plan, one persistent hash launch over all matrices' chunks and
+// finalize.  plan.spl/minb/ntiles/grid select the hash variant; plan_threads
+// is the sum of rows+1 over the matrices that have rows.
+cudaError_t launch_batch(const BatchArgs &b, const HashPlan &plan, uint32_t plan_threads,
+                         cudaStream_t stream);
+// Blocks per SM the hash kernel variant launched for (samples per lane,
+// register budget, s_pad) reaches, and its registers per thread.
+int hash_blocks_per_sm(uint32_t spl, uint32_t minb, uint32_t s_pad);
+size_t hash_kernel_registers(uint32_t spl, uint32_t minb, uint32_t s_pad);
 
 // Parameter kernels (param_kernels.cu).
 enum class PairOp : int { kGamma = 0, kLogGamma = 1, kCopy = 2 };
@@ -97,6 +137,26 @@ void stream_copy(void *dst, const void *src, size_t bytes);
 // [0, 2^32) become 0xFFFFFFFF), with non-temporal stores for large pieces.
 void convert_f64_to_f32(float *dst, const double *src, size_t n);
 void convert_i64_to_u32(uint32_t *dst, const uint64_t *src, size_t n);
+
+// Makes `device` current for the calling thread while the guard lives and
+// then gives the thread back the state it came with: its previous device, or
+// no current context at all when it had none (restoring "device 0" there
+// would create a context on device 0 that the caller never asked for).
+// Every extern "C" entry point that works on a device holds one.
+class DeviceGuard {
+ public:
+  explicit DeviceGuard(int device);
+  ~DeviceGuard();
+  DeviceGuard(const DeviceGuard &) = delete;
+  DeviceGuard &operator=(const DeviceGuard &) = delete;
+  bool ok() const { return ok_; }
+
+ private:
+  int prev_ = -1;
+  bool had_context_ = true;
+  bool changed_ = false;
+  bool ok_ = false;
+};
 
 // Read-only view of a generator's fields for entry points that live outside
 // engine.cu (engine.cu).

@@ -135,6 +135,23 @@ def host_csr(w: Workload, row0: int, rows: int, device="cuda"):
             weights[:nnz].cpu().numpy())
 
 
+def small_csr(seed: int = 1):
+    """The small configuration's 6400 x 130 float32 CSR: uniform integers
+    0..99, each kept where a second uniform integer 0..4 is >= 4 (~80% zeros),
+    drawn with numpy's legacy RandomState(seed) in that order (the reference
+    tests' matrix, test.py:35-39 / 93-97).  Returns (indptr, cols, weights) as
+    uint32 / uint32 / float32 numpy arrays."""
+    rng = np.random.RandomState(seed)
+    data = rng.randint(0, 100, (6400, 130))
+    mask = rng.randint(0, 5, data.shape)
+    data = (data * (mask >= 4)).astype(np.float32)
+    nz = data != 0
+    indptr = np.zeros(data.shape[0] + 1, np.uint32)
+    np.cumsum(nz.sum(axis=1), out=indptr[1:])
+    cols = np.nonzero(nz)[1].astype(np.uint32)
+    return indptr, cols, data[nz].astype(np.float32)
+
+
 def batched_shapes(w: Workload):
     """Row counts of the batched workload's matrices: floor(exp(U(0, ln 4096)))
     clipped to [1, 4096], seeded."""

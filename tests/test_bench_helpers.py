@@ -34,3 +34,40 @@ def test_srpt_ideal_small_jobs_preempt_large_ones():
     hi = b.srpt_ideal(sizes, rate=1e12, load=0.8, seed=2)
     assert abs(lo["p50_ms"] - 1e-3) < 1e-6 and abs(hi["p50_ms"] - 1e-3) < 1e-6
     assert hi["p99_ms"] > lo["p99_ms"] >= 1.0 - 1e-9
+
+
+def test_hash_roofline_picks_the_binding_resource():
+    """The roofline reports DRAM, issue and the FP32 floor side by side and
+    names the one closest to its peak; the algorithmic-byte rate is kept
+    beside them."""
+    b = _bench()
+    prof = {"dram_bytes_per_eval": 4.0, "thread_inst_per_eval": 20.0, "captured_case": "x"}
+    nnz, R, S = 1_000_000_000, 1_000_000, 128
+    evals = nnz * S
+    t_ms = 200.0
+    r = b.hash_roofline(nnz, R, S, t_ms, 1500.0, 6500.0, "measured", prof, True)
+    dram = 4.0 * evals / (t_ms / 1e3) / 1e9 / 6500.0
+    issue = 20.0 * evals / (t_ms / 1e3) / (148 * 128 * 1500e6)
+    assert abs(r["dram"]["frac"] - dram) < 1e-9 and abs(r["issue"]["frac"] - issue) < 1e-9
+    assert r["bound"] == ("issue" if issue > dram else "hbm")
+    assert r["frac"] == max(dram, issue)
+    assert abs(r["fp32_floor"]["frac"] - issue * 8 / 20) < 1e-9
+    alg = 12 * nnz * S + 8 * nnz + 4 * (R + 1) + 8 * R * S
+    assert abs(r["algorithmic_frac"] - alg / (t_ms / 1e3) / 1e9 / 6500.0) < 1e-9
+    assert r["traffic"] == 4.0 * evals
+    # Without counters only the algorithmic HBM bound is left.
+    r2 = b.hash_roofline(nnz, R, S, t_ms, None, 6500.0, "measured", None, False)
+    assert r2["bound"] == "hbm" and r2["traffic"] is None
+
+
+def test_small_config_matrix_matches_the_oracle_restatement():
+    """bench's small configuration matrix is the reference tests' 6400x130
+    matrix."""
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from minhashcuda_b200 import synth
+    ip, cols, w = synth.small_csr(1)
+    _, m = O.reference_small_matrix(1)
+    assert np.array_equal(ip, m.indptr) and np.array_equal(cols, m.indices)
+    assert np.array_equal(w, m.data)
