@@ -12,6 +12,7 @@
 //  - grow-only device workspace as in minhashcuda.cc:385-455, but sizes and
 //    offsets are 64-bit and every launch is checked.
 #include <algorithm>
+#include <atomic>
 #include <cinttypes>
 #include <cstdarg>
 #include <cstdio>
@@ -506,7 +507,7 @@ void par_for(size_t n, size_t split, F f) {
 // to nearest; a 64-bit column outside [0, 2^32) becomes 0xFFFFFFFF, which no
 // dim admits, so the device check rejects it instead of a wrapped value
 // passing.
-void stage_entries(const HostCsr &in, uint64_t b0, size_t n, float *w, uint32_t *c) {
+void stage_weights(const HostCsr &in, uint64_t b0, size_t n, float *w) {
   constexpr size_t kSplit = size_t{2} << 20;
   if (in.w64) {
     const double *src = static_cast<const double *>(in.weights) + b0;
@@ -514,6 +515,10 @@ void stage_entries(const HostCsr &in, uint64_t b0, size_t n, float *w, uint32_t 
   } else {
     par_memcpy(w, static_cast<const float *>(in.weights) + b0, n * sizeof(float));
   }
+}
+
+void stage_cols(const HostCsr &in, uint64_t b0, size_t n, uint32_t *c) {
+  constexpr size_t kSplit = size_t{2} << 20;
   if (in.cols64) {
     // int64 and uint64 alike: a negative int64 has its high bits set.
     const uint64_t *src = static_cast<const uint64_t *>(in.cols) + b0;
@@ -522,6 +527,26 @@ void stage_entries(const HostCsr &in, uint64_t b0, size_t n, float *w, uint32_t 
     par_memcpy(c, static_cast<const uint32_t *>(in.cols) + b0, n * sizeof(uint32_t));
   }
 }
+
+// Packs the caller's 32-bit columns [b0, b0 + n) into page-locked lo/hi
+// arrays (mhb::pack_cols, split over host threads at even entries).  Returns
+// false if some column needs more than 16 + hi_bits bits; the block then
+// crosses the link unpacked.
+bool stage_packed_cols(const HostCsr &in, uint64_t b0, size_t n, uint16_t *lo, uint8_t *hi,
+                       int hi_bits) {
+  constexpr size_t kSplit = size_t{2} << 20;
+  const uint32_t *src = static_cast<const uint32_t *>(in.cols) + b0;
+  std::atomic<bool> fits{true};
+  par_for(n, kSplit, [&, src, lo, hi](size_t b, size_t e) {
+    if (!mhb::pack_cols(src + b, e - b, lo + b, hi + (hi_bits == 4 ? b / 2 : b), hi_bits))
+      fits.store(false, std::memory_order_relaxed);
+  });
+  return fits.load();
+}
+
+// Byte offset of the high parts behind `n` low halves in a packed-column
+// buffer (16-byte aligned for the kernel's bulk copies).
+size_t packed_hi_offset(size_t n) { return (2 * n + 255) & ~static_cast<size_t>(255); }
 
 MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
                             uint32_t *output) {
@@ -534,6 +559,12 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
   const bool pin_in = in.native() && is_pinned(in.weights) && is_pinned(in.cols) &&
                       is_pinned(rows);
   const bool pin_out = is_pinned(output);
+  // 32-bit columns cross the host link packed when dim allows it: 16 low
+  // bits plus 4 (dim <= 2^20) or 8 (dim <= 2^24) high bits, 6.5 or 7 bytes
+  // per entry with the weight instead of 8 (the link bounds this path).
+  const int pack_bits = (in.cols64 == 0 && env_int("MHCUDA_B200_NO_PACK", 0) == 0)
+                            ? (gen->dim <= (1u << 20) ? 4 : (gen->dim <= (1u << 24) ? 8 : 0))
+                            : 0;
   // Page-locked inputs copy straight from the caller: large blocks.  Pageable
   // ones go through pinned staging, which is cheaper to allocate (and
   // re-fill) in smaller blocks.
@@ -618,14 +649,15 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
     for (int k = 0; k < Gen::kPipeSlots; ++k) {
       Gen::Slot &sl = gen->slots[k];
       MHB_CHECK(gen, sl.w.ensure(max_n * 4 + 16), mhcudaMemoryAllocationFailure);
-      MHB_CHECK(gen, sl.c.ensure(max_n * 4 + 16), mhcudaMemoryAllocationFailure);
+      MHB_CHECK(gen, sl.c.ensure(max_n * 4 + 512), mhcudaMemoryAllocationFailure);
       MHB_CHECK(gen, sl.ip.ensure((max_len + 1) * 4), mhcudaMemoryAllocationFailure);
       MHB_CHECK(gen, sl.out.ensure(max_len * row_bytes), mhcudaMemoryAllocationFailure);
       if (!pin_in) {
         MHB_CHECK(gen, sl.hw.ensure(max_n * 4), mhcudaMemoryAllocationFailure);
-        MHB_CHECK(gen, sl.hc.ensure(max_n * 4), mhcudaMemoryAllocationFailure);
         MHB_CHECK(gen, sl.hip.ensure((max_len + 1) * 4), mhcudaMemoryAllocationFailure);
       }
+      if (!pin_in || pack_bits)
+        MHB_CHECK(gen, sl.hc.ensure(max_n * 4 + 512), mhcudaMemoryAllocationFailure);
       if (!pin_out) MHB_CHECK(gen, sl.hout.ensure(max_len * row_bytes), mhcudaMemoryAllocationFailure);
     }
     HashPlan big{};
@@ -645,19 +677,26 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
     const uint32_t b0 = rows[r0];
     const uint32_t n = rows[r1] - b0;
     MHB_CHECK(gen, sl.w.ensure(static_cast<size_t>(n) * 4 + 16), mhcudaMemoryAllocationFailure);
-    MHB_CHECK(gen, sl.c.ensure(static_cast<size_t>(n) * 4 + 16), mhcudaMemoryAllocationFailure);
+    MHB_CHECK(gen, sl.c.ensure(static_cast<size_t>(n) * 4 + 512), mhcudaMemoryAllocationFailure);
     MHB_CHECK(gen, sl.ip.ensure((static_cast<size_t>(len) + 1) * 4), mhcudaMemoryAllocationFailure);
     MHB_CHECK(gen, sl.out.ensure(len * row_bytes), mhcudaMemoryAllocationFailure);
     const void *src_w = nullptr, *src_c = nullptr, *src_i = rows + r0;
+    if (!pin_in || pack_bits)
+      MHB_CHECK(gen, sl.hc.ensure(static_cast<size_t>(n) * 4 + 512), mhcudaMemoryAllocationFailure);
+    const size_t hi_off = packed_hi_offset(n);
+    const size_t hi_bytes = pack_bits == 4 ? (static_cast<size_t>(n) + 1) / 2 : n;
+    const bool packed =
+        pack_bits && n &&
+        stage_packed_cols(in, b0, n, sl.hc.as<uint16_t>(), sl.hc.as<uint8_t>() + hi_off, pack_bits);
     if (pin_in) {
       src_w = static_cast<const float *>(in.weights) + b0;
       src_c = static_cast<const uint32_t *>(in.cols) + b0;
     } else {
       MHB_CHECK(gen, sl.hw.ensure(static_cast<size_t>(n) * 4), mhcudaMemoryAllocationFailure);
-      MHB_CHECK(gen, sl.hc.ensure(static_cast<size_t>(n) * 4), mhcudaMemoryAllocationFailure);
       MHB_CHECK(gen, sl.hip.ensure((static_cast<size_t>(len) + 1) * 4),
                 mhcudaMemoryAllocationFailure);
-      stage_entries(in, b0, n, static_cast<float *>(sl.hw.ptr), static_cast<uint32_t *>(sl.hc.ptr));
+      stage_weights(in, b0, n, static_cast<float *>(sl.hw.ptr));
+      if (!packed) stage_cols(in, b0, n, static_cast<uint32_t *>(sl.hc.ptr));
       memcpy(sl.hip.ptr, src_i, (static_cast<size_t>(len) + 1) * 4);
       src_w = sl.hw.ptr;
       src_c = sl.hc.ptr;
@@ -670,9 +709,18 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
       MHB_CHECK(gen, cudaMemcpyAsync(sl.w.ptr, src_w, static_cast<size_t>(n) * 4,
                                      cudaMemcpyHostToDevice, gen->s_in),
                 mhcudaMemoryCopyError);
-      MHB_CHECK(gen, cudaMemcpyAsync(sl.c.ptr, src_c, static_cast<size_t>(n) * 4,
-                                     cudaMemcpyHostToDevice, gen->s_in),
-                mhcudaMemoryCopyError);
+      if (packed) {
+        MHB_CHECK(gen, cudaMemcpyAsync(sl.c.ptr, sl.hc.ptr, static_cast<size_t>(n) * 2,
+                                       cudaMemcpyHostToDevice, gen->s_in),
+                  mhcudaMemoryCopyError);
+        MHB_CHECK(gen, cudaMemcpyAsync(sl.c.as<char>() + hi_off, sl.hc.as<char>() + hi_off,
+                                       hi_bytes, cudaMemcpyHostToDevice, gen->s_in),
+                  mhcudaMemoryCopyError);
+      } else {
+        MHB_CHECK(gen, cudaMemcpyAsync(sl.c.ptr, src_c, static_cast<size_t>(n) * 4,
+                                       cudaMemcpyHostToDevice, gen->s_in),
+                  mhcudaMemoryCopyError);
+      }
     }
     MHB_CHECK(gen, cudaEventRecord(sl.h2d, gen->s_in), mhcudaRuntimeError);
     MHB_CHECK(gen, cudaStreamWaitEvent(st, sl.h2d, 0), mhcudaRuntimeError);
@@ -681,7 +729,13 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
     r = prepare_launch(gen, len, n, plan, &a);
     if (r != mhcudaSuccess) break;
     a.weights = sl.w.as<float>();
-    a.cols = sl.c.as<uint32_t>();
+    if (packed) {
+      a.cols_lo = sl.c.as<uint16_t>();
+      a.cols_hi = sl.c.as<uint8_t>() + hi_off;
+      a.col_hi_bits = static_cast<uint32_t>(pack_bits);
+    } else {
+      a.cols = sl.c.as<uint32_t>();
+    }
     a.indptr = sl.ip.as<uint32_t>();
     a.out = sl.out.as<uint32_t>();
     r = enqueue_hash(gen, a, plan, st, /*clear_status=*/false);

@@ -129,6 +129,13 @@ __device__ __forceinline__ void wmh_update(float t, float r, float c, float b, u
   pos = lt ? p : pos;
 }
 
+// Column of relative position p in a packed CSR.
+__device__ __forceinline__ uint32_t packed_col(const HashArgs &a, uint32_t p) {
+  const uint32_t h = a.col_hi_bits == 4 ? (a.cols_hi[p >> 1] >> ((p & 1u) * 4)) & 15u
+                                        : a.cols_hi[p];
+  return static_cast<uint32_t>(a.cols_lo[p]) | (h << 16);
+}
+
 // The output pair of kernel.cu:108 for sample s whose minimum came from the
 // entry at relative position `pos`: k = cols[pos] and t recomputed from the
 // entry with the exact quotient.  Every evaluation used that same t (fast_t
@@ -139,7 +146,7 @@ __device__ __forceinline__ void wmh_update(float t, float r, float c, float b, u
 // left unwritten) yields kNone and reads nothing.
 __device__ __forceinline__ uint2 resolve(const HashArgs &a, uint32_t pos, uint32_t s) {
   if (pos >= a.nnz) return make_uint2(kNone, kNone);
-  const uint32_t k = a.cols[pos];
+  const uint32_t k = a.col_hi_bits ? packed_col(a, pos) : a.cols[pos];
   // An invalid column was evaluated as column 0 and failed the call: keep
   // the parameter reads in bounds.
   if (k >= a.dim) return make_uint2(kNone, kNone);
@@ -234,6 +241,15 @@ struct alignas(16) WarpStage {
   unsigned long long bar[2];
 };
 
+// Landing area of packed columns (HashArgs::col_hi_bits != 0): the low 16
+// bits and the high nibbles or bytes of each window's columns, rebuilt into
+// WarpStage::c by finish_window.
+struct alignas(16) PackedStage {
+  uint16_t lo[2][kWin];
+  uint8_t hi[2][kWin];
+};
+
+
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
@@ -285,22 +301,40 @@ __device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, uint32
 #endif
 }
 
+// Positions of a window that arrive by bulk copy: a multiple of 4 (16 bytes
+// of weights and of columns), or of 32 with packed columns (16 bytes of high
+// nibbles); window starts are multiples of 32.
+template <bool PACKED>
+__device__ __forceinline__ uint32_t bulk_positions(uint32_t n, bool bulk_ok) {
+  return bulk_ok ? (n & (PACKED ? ~31u : ~3u)) : 0u;
+}
+
 // Lane 0 starts the copy of positions [ws, ws + n) into buffer `b`: the
-// 16-byte-aligned body by two bulk copies, the ragged tail is left to
+// 16-byte-aligned body by bulk copies, the ragged tail is left to
 // finish_window's plain loads.
-__device__ __forceinline__ void issue_window(const HashArgs &a, WarpStage &st, uint32_t b,
-                                             uint32_t ws, uint32_t n, bool bulk_ok,
+template <bool PACKED>
+__device__ __forceinline__ void issue_window(const HashArgs &a, WarpStage &st, PackedStage *pk,
+                                             uint32_t b, uint32_t ws, uint32_t n, bool bulk_ok,
                                              uint32_t lane) {
   // Order this warp's earlier generic accesses of the buffer before the
   // asynchronous writes that are about to land in it.
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   __syncwarp();
   if (lane == 0) {
-    const uint32_t nb = bulk_ok ? (n & ~3u) : 0u;
+    const uint32_t nb = bulk_positions<PACKED>(n, bulk_ok);
     if (nb) {
-      mbar_arrive_expect_tx(&st.bar[b], 8u * nb);
-      bulk_copy_g2s(st.w[b], a.weights + ws, 4u * nb, &st.bar[b]);
-      bulk_copy_g2s(st.c[b], a.cols + ws, 4u * nb, &st.bar[b]);
+      if constexpr (PACKED) {
+        const uint32_t hi_bytes = a.col_hi_bits == 4 ? nb / 2 : nb;
+        const uint32_t hi_off = a.col_hi_bits == 4 ? ws / 2 : ws;
+        mbar_arrive_expect_tx(&st.bar[b], 6u * nb + hi_bytes);
+        bulk_copy_g2s(st.w[b], a.weights + ws, 4u * nb, &st.bar[b]);
+        bulk_copy_g2s(pk->lo[b], a.cols_lo + ws, 2u * nb, &st.bar[b]);
+        bulk_copy_g2s(pk->hi[b], a.cols_hi + hi_off, hi_bytes, &st.bar[b]);
+      } else {
+        mbar_arrive_expect_tx(&st.bar[b], 8u * nb);
+        bulk_copy_g2s(st.w[b], a.weights + ws, 4u * nb, &st.bar[b]);
+        bulk_copy_g2s(st.c[b], a.cols + ws, 4u * nb, &st.bar[b]);
+      }
     } else {
       mbar_arrive(&st.bar[b]);
     }
@@ -313,19 +347,30 @@ __device__ __forceinline__ void issue_window(const HashArgs &a, WarpStage &st, u
 // hashes are not valid output) and is replaced by column 0, so the
 // evaluation loop reads only in-bounds parameters without a check per nnz.
 // Returns false if the copy did not complete within the spin limit.
-__device__ __forceinline__ bool finish_window(const HashArgs &a, WarpStage &st, uint32_t b,
-                                              uint32_t parity, uint32_t ws, uint32_t n,
-                                              bool bulk_ok, uint32_t lane) {
+template <bool PACKED>
+__device__ __forceinline__ bool finish_window(const HashArgs &a, WarpStage &st, PackedStage *pk,
+                                              uint32_t b, uint32_t parity, uint32_t ws,
+                                              uint32_t n, bool bulk_ok, uint32_t lane) {
   uint32_t spins = 0;
   while (!mbar_try_wait(&st.bar[b], parity)) {
     if (++spins > kSpinLimit) return false;
   }
-  const uint32_t nb = bulk_ok ? (n & ~3u) : 0u;
+  const uint32_t nb = bulk_positions<PACKED>(n, bulk_ok);
   bool bad = false;
   for (uint32_t i = lane; i < n; i += 32) {
     float x;
     uint32_t col;
-    if (i < nb) {
+    if constexpr (PACKED) {
+      if (i < nb) {
+        x = st.w[b][i];
+        const uint32_t h = a.col_hi_bits == 4 ? (pk->hi[b][i >> 1] >> ((i & 1u) * 4)) & 15u
+                                              : pk->hi[b][i];
+        col = static_cast<uint32_t>(pk->lo[b][i]) | (h << 16);
+      } else {
+        x = __ldg(a.weights + ws + i);
+        col = packed_col(a, ws + i);
+      }
+    } else if (i < nb) {
       x = st.w[b][i];
       col = st.c[b][i];
     } else if (a.host_csr) {  // mapped host memory: plain loads
@@ -483,14 +528,17 @@ __device__ __forceinline__ void eval_all(const Params<SPL> &p, float w, uint32_t
 // phases and the launch-wide constants of the item loop.
 struct WarpCtx {
   WarpStage *stg;
+  PackedStage *pk;  // packed-column landing area (packed kernels only)
   uint32_t parity;  // bit b: phase parity to wait for on buffer b
   uint32_t lane;
   uint64_t pol;     // L2 policy of the parameter loads
 };
 
-__device__ __forceinline__ void warp_ctx_init(WarpCtx &w, WarpStage *stage_all) {
+__device__ __forceinline__ void warp_ctx_init(WarpCtx &w, WarpStage *stage_all,
+                                              PackedStage *packed_all = nullptr) {
   w.lane = threadIdx.x & 31u;
   w.stg = &stage_all[threadIdx.x >> 5];
+  w.pk = packed_all ? &packed_all[threadIdx.x >> 5] : nullptr;
   if (w.lane == 0) {
     mbar_init(&w.stg->bar[0], 1);
     mbar_init(&w.stg->bar[1], 1);
@@ -512,19 +560,23 @@ __device__ __forceinline__ void warp_ctx_init(WarpCtx &w, WarpStage *stage_all) 
 // SPAD: the generator's s_pad when it is known at compile time (0: read it
 // from the arguments), which turns the parameter-block addressing into one
 // wide multiply-add and immediate load offsets.
-template <int SPL, int SPAD>
+template <int SPL, int SPAD, bool PACKED>
 __device__ __forceinline__ bool hash_item(const HashArgs &a, uint32_t c, uint32_t tile,
                                           WarpCtx &wc) {
   const uint32_t lane = wc.lane;
   WarpStage &stg = *wc.stg;
+  PackedStage *pk = wc.pk;
   uint32_t &parity = wc.parity;
   const uint64_t pol = wc.pol;
   const uint32_t base = a.indptr[0];
   const uint32_t spad = SPAD ? static_cast<uint32_t>(SPAD) : a.s_pad;
   const size_t col_stride = static_cast<size_t>(3) * (SPAD ? static_cast<uint32_t>(SPAD) : a.s_pad);
   // Bulk copies only from device memory; mapped host CSR is read by the lanes.
-  const bool bulk_ok = !a.host_csr && ((reinterpret_cast<uintptr_t>(a.weights) |
-                                        reinterpret_cast<uintptr_t>(a.cols)) & 15u) == 0;
+  const uintptr_t col_addr =
+      PACKED ? (reinterpret_cast<uintptr_t>(a.cols_lo) | reinterpret_cast<uintptr_t>(a.cols_hi))
+             : reinterpret_cast<uintptr_t>(a.cols);
+  const bool bulk_ok =
+      !a.host_csr && ((reinterpret_cast<uintptr_t>(a.weights) | col_addr) & 15u) == 0;
   {
     const uint32_t s0 = tile * (32u * SPL) + lane * SPL;
     const bool active = s0 < spad;
@@ -563,8 +615,9 @@ __device__ __forceinline__ bool hash_item(const HashArgs &a, uint32_t c, uint32_
     };
 
     const uint32_t nwin = (ce - cs + kWin - 1) / kWin;
-    if (nwin > 0) issue_window(a, stg, 0, cs, min(kWin, ce - cs), bulk_ok, lane);
-    if (nwin > 1) issue_window(a, stg, 1, cs + kWin, min(kWin, ce - cs - kWin), bulk_ok, lane);
+    if (nwin > 0) issue_window<PACKED>(a, stg, pk, 0, cs, min(kWin, ce - cs), bulk_ok, lane);
+    if (nwin > 1)
+      issue_window<PACKED>(a, stg, pk, 1, cs + kWin, min(kWin, ce - cs - kWin), bulk_ok, lane);
 
     // Error exits wait (bounded) for the windows still in flight into this
     // warp's staging buffers before leaving: windows [from, min(from+2, nwin)).
@@ -581,7 +634,7 @@ __device__ __forceinline__ bool hash_item(const HashArgs &a, uint32_t c, uint32_
       const uint32_t b = k & 1u;
       const uint32_t ws = cs + k * kWin;
       const uint32_t n = min(kWin, ce - ws);
-      if (!finish_window(a, stg, b, (parity >> b) & 1u, ws, n, bulk_ok, lane)) {
+      if (!finish_window<PACKED>(a, stg, pk, b, (parity >> b) & 1u, ws, n, bulk_ok, lane)) {
         if (lane == 0) atomicOr(a.status, kStatusStall);
         drain(k);
         return false;
@@ -633,7 +686,7 @@ __device__ __forceinline__ bool hash_item(const HashArgs &a, uint32_t c, uint32_
       }
       if (k + 2 < nwin) {
         const uint32_t ws2 = ws + 2 * kWin;
-        issue_window(a, stg, b, ws2, min(kWin, ce - ws2), bulk_ok, lane);
+        issue_window<PACKED>(a, stg, pk, b, ws2, min(kWin, ce - ws2), bulk_ok, lane);
       }
     }
     flush();
@@ -650,18 +703,24 @@ __device__ __forceinline__ bool hash_item(const HashArgs &a, uint32_t c, uint32_
   return true;
 }
 
-template <int SPL, int MINB, int SPAD>
+// PACKED: the columns arrive as cols_lo/cols_hi (HashArgs::col_hi_bits).
+template <int SPL, int MINB, int SPAD, bool PACKED>
 __global__ void __launch_bounds__(kHashBlock, MINB) hash_kernel(const HashArgs a) {
   __shared__ WarpStage stage_all[kHashBlock / 32];
+  PackedStage *packed_all = nullptr;
+  if constexpr (PACKED) {
+    __shared__ PackedStage packed_stage[kHashBlock / 32];
+    packed_all = packed_stage;
+  }
   if (*a.status & kStatusBadIndptr) return;
   WarpCtx wc;
-  warp_ctx_init(wc, stage_all);
+  warp_ctx_init(wc, stage_all, packed_all);
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
   const uint32_t items = a.nchunks * a.ntiles;
   for (uint32_t item = gw; item < items; item += nw) {
     const uint32_t c = item / a.ntiles;
-    if (!hash_item<SPL, SPAD>(a, c, item - c * a.ntiles, wc)) return;
+    if (!hash_item<SPL, SPAD, PACKED>(a, c, item - c * a.ntiles, wc)) return;
   }
 }
 
@@ -908,7 +967,7 @@ __global__ void __launch_bounds__(kHashBlock, MINB) hash_batch_kernel(const Batc
     __syncwarp();
     if (wc.lane == 0) view = matrix_view(b, b.mats[m], chunk);
     __syncwarp();
-    if (!hash_item<SPL, SPAD>(view, gc - base, item - gc * ntiles, wc)) return;
+    if (!hash_item<SPL, SPAD, false>(view, gc - base, item - gc * ntiles, wc)) return;
   }
 }
 
@@ -974,24 +1033,33 @@ BatchFn pick_batch(uint32_t spl, uint32_t minb, uint32_t s_pad) {
 
 // Instantiated (samples per lane, minimum resident blocks per SM) variants,
 // with s_pad compiled in for the common sample counts.
-HashFn pick_hash(uint32_t spl, uint32_t minb, uint32_t s_pad) {
+HashFn pick_hash(uint32_t spl, uint32_t minb, uint32_t s_pad, bool packed = false) {
+  if (packed) {
+    switch (spl * 10 + minb) {
+      case 44: return hash_kernel<4, 4, 0, true>;
+      case 43: return hash_kernel<4, 3, 0, true>;
+      case 24: return hash_kernel<2, 4, 0, true>;
+      case 14: return hash_kernel<1, 4, 0, true>;
+      default: return nullptr;
+    }
+  }
 #if MHB_SPAD_TEMPLATES
   switch (spl * 100000 + minb * 10000 + s_pad) {
-    case 440128: return hash_kernel<4, 4, 128>;
-    case 430128: return hash_kernel<4, 3, 128>;
-    case 440256: return hash_kernel<4, 4, 256>;
-    case 430256: return hash_kernel<4, 3, 256>;
-    case 240064: return hash_kernel<2, 4, 64>;
+    case 440128: return hash_kernel<4, 4, 128, false>;
+    case 430128: return hash_kernel<4, 3, 128, false>;
+    case 440256: return hash_kernel<4, 4, 256, false>;
+    case 430256: return hash_kernel<4, 3, 256, false>;
+    case 240064: return hash_kernel<2, 4, 64, false>;
     default: break;
   }
 #else
   (void)s_pad;
 #endif
   switch (spl * 10 + minb) {
-    case 44: return hash_kernel<4, 4, 0>;
-    case 43: return hash_kernel<4, 3, 0>;
-    case 24: return hash_kernel<2, 4, 0>;
-    case 14: return hash_kernel<1, 4, 0>;
+    case 44: return hash_kernel<4, 4, 0, false>;
+    case 43: return hash_kernel<4, 3, 0, false>;
+    case 24: return hash_kernel<2, 4, 0, false>;
+    case 14: return hash_kernel<1, 4, 0, false>;
     default: return nullptr;
   }
 }
@@ -999,7 +1067,7 @@ HashFn pick_hash(uint32_t spl, uint32_t minb, uint32_t s_pad) {
 }  // namespace
 
 cudaError_t launch_hash(const HashArgs &a, const HashPlan &plan, cudaStream_t stream) {
-  const HashFn fn = pick_hash(plan.spl, plan.minb, a.s_pad);
+  const HashFn fn = pick_hash(plan.spl, plan.minb, a.s_pad, a.col_hi_bits != 0);
   if (!fn) return cudaErrorInvalidValue;
   fn<<<plan.grid, kHashBlock, 0, stream>>>(a);
   return cudaGetLastError();

@@ -39,6 +39,7 @@
 #include <deque>
 #include <memory>
 #include <mutex>
+#include <string>
 #include <thread>
 #include <unordered_map>
 #include <vector>
@@ -61,6 +62,10 @@ struct Request {
   uint32_t length = 0;
   uint32_t *output = nullptr;
   Clock::time_point submitted, finished;
+  // Stage times for tracing (MHCUDA_B200_SERVER_TRACE): first row taken by a
+  // lane, last unit's launches enqueued, last unit's device work done.
+  Clock::time_point taken, launched, gpu_done;
+  bool was_taken = false;
   uint32_t next_row = 0;        // first row not yet handed to a lane
   uint32_t inflight = 0;        // units handed out and not yet complete
   bool in_pinned = false;       // weights and cols are page-locked: large units copy directly
@@ -129,6 +134,10 @@ struct MinhashCudaServer_ {
   std::deque<Request *> ring;        // requests with rows not yet handed out
   std::unordered_map<uint64_t, std::unique_ptr<Request>> requests;
   std::vector<double> latencies_ms;  // completed requests, for mhcuda_server_stats
+  // Per-request stage trace, written as CSV at stop when
+  // MHCUDA_B200_SERVER_TRACE names a file.
+  std::string trace_path;
+  std::vector<std::string> trace;
   uint64_t next_ticket = 1;
   uint64_t evals_done = 0;
   Clock::time_point stats_since = Clock::now();
@@ -201,6 +210,14 @@ MinhashCudaServer_::~MinhashCudaServer_() {
   work.notify_all();
   for (Lane &l : lanes)
     if (l.thread.joinable()) l.thread.join();
+  if (!trace_path.empty()) {
+    if (FILE *f = fopen(trace_path.c_str(), "w")) {
+      fprintf(f, "ticket,samples,rows,nnz,queued_ms,gather_launch_ms,device_ms,complete_ms,"
+                 "total_ms\n");
+      for (const std::string &line : trace) fprintf(f, "%s\n", line.c_str());
+      fclose(f);
+    }
+  }
   mhb::DeviceGuard on_device(device);
   for (Lane &l : lanes) {
     if (l.stream) cudaStreamSynchronize(l.stream);
@@ -362,6 +379,18 @@ void MinhashCudaServer_::finish_locked(Request *r, Clock::time_point now) {
   r->finished = now;
   if (!r->cancelled)
     latencies_ms.push_back(std::chrono::duration<double, std::milli>(now - r->submitted).count());
+  if (!trace_path.empty() && !r->cancelled && r->was_taken) {
+    auto ms = [](Clock::time_point a, Clock::time_point b) {
+      return std::chrono::duration<double, std::milli>(b - a).count();
+    };
+    char line[256];
+    snprintf(line, sizeof(line), "%llu,%u,%u,%llu,%.4f,%.4f,%.4f,%.4f,%.4f",
+             static_cast<unsigned long long>(r->ticket), r->g.samples, r->length,
+             static_cast<unsigned long long>(r->rows[r->length] - r->rows[0]),
+             ms(r->submitted, r->taken), ms(r->taken, r->launched), ms(r->launched, r->gpu_done),
+             ms(r->gpu_done, now), ms(r->submitted, now));
+    trace.emplace_back(line);
+  }
 }
 
 // Under `mu`: fills lane.units shortest-remaining-work first.  Requests are
@@ -425,6 +454,10 @@ bool MinhashCudaServer_::take(Lane &lane) {
     }
     if (r1 == r->next_row) continue;  // not even one row fits what is left
     if (!allow_low && r1 < r->length) break;  // would not finish in this batch
+    if (!r->was_taken) {
+      r->was_taken = true;
+      r->taken = Clock::now();
+    }
     batch.push_back(Unit{r, r->next_row, r1});
     r->next_row = r1;
     ++r->inflight;
@@ -499,9 +532,18 @@ void MinhashCudaServer_::lane_loop(Lane &lane) {
       }
     }
     MHCUDAResult r = run_units(lane, lane.units, false);
+    const Clock::time_point launched = Clock::now();
     if (r == mhcudaSuccess && cudaEventSynchronize(lane.done_ev) != cudaSuccess) {
       cudaGetLastError();
       r = mhcudaRuntimeError;
+    }
+    if (!trace_path.empty()) {
+      const Clock::time_point done = Clock::now();
+      std::lock_guard<std::mutex> lock(mu);
+      for (const Unit &u : lane.units) {
+        u.req->launched = launched;
+        u.req->gpu_done = done;
+      }
     }
     complete(lane, r);
   }
@@ -543,6 +585,7 @@ MinhashCudaServer *mhcuda_server_start(uint32_t devices, uint64_t hbm_budget_byt
   srv->max_unit_evals = env_u64("MHCUDA_B200_SERVER_UNIT_EVALS", srv->max_unit_evals);
   srv->max_batch_evals = env_u64("MHCUDA_B200_SERVER_BATCH_EVALS", srv->max_batch_evals);
   srv->zero_copy_max_bytes = env_u64("MHCUDA_B200_SERVER_ZERO_COPY_MAX_BYTES", ~0ull);
+  if (const char *tp = getenv("MHCUDA_B200_SERVER_TRACE")) srv->trace_path = tp;
   srv->max_low_inflight = static_cast<uint32_t>(std::min<uint64_t>(
       lanes, env_u64("MHCUDA_B200_SERVER_LOW_INFLIGHT", lanes > 2 ? lanes - 2 : 1)));
   cudaDeviceGetAttribute(&srv->sm_count, cudaDevAttrMultiProcessorCount, dev);

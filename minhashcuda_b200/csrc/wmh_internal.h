@@ -67,6 +67,13 @@ struct HashArgs {
   uint32_t *out;             // [rows][samples][2]
   uint32_t *status;          // device status word
   uint32_t host_csr;         // weights/cols/indptr/out are mapped host memory
+  // Packed columns (col_hi_bits 4 or 8; cols unused): column p is
+  // cols_lo[p] | hi(p) << 16, hi(p) the nibble p of cols_hi (4: entry p in
+  // byte p/2, low nibble for even p) or its byte p (8).  Device memory, both
+  // arrays 16-byte aligned.  col_hi_bits 0: the columns are `cols`.
+  const uint16_t *cols_lo;
+  const uint8_t *cols_hi;
+  uint32_t col_hi_bits;
 };
 
 // One matrix of a device-resident batch (mhcuda_calc_batch_device).  The
@@ -137,6 +144,12 @@ void stream_copy(void *dst, const void *src, size_t bytes);
 // [0, 2^32) become 0xFFFFFFFF), with non-temporal stores for large pieces.
 void convert_f64_to_f32(float *dst, const double *src, size_t n);
 void convert_i64_to_u32(uint32_t *dst, const uint64_t *src, size_t n);
+// Packed columns for the host->device link: lo[i] = low 16 bits of src[i],
+// hi = the bits above, as bytes (hi_bits 8: hi[i]) or nibbles (hi_bits 4:
+// entry i in byte i/2, the low nibble for even i).  Returns false if some
+// column needs more than 16 + hi_bits bits.  A range split across calls must
+// be split at even entries.
+bool pack_cols(const uint32_t *src, size_t n, uint16_t *lo, uint8_t *hi, int hi_bits);
 
 // Makes `device` current for the calling thread while the guard lives and
 // then gives the thread back the state it came with: its previous device, or

@@ -14,6 +14,7 @@ namespace mhb {
 void stream_copy(void *dst, const void *src, size_t bytes);
 void convert_f64_to_f32(float *dst, const double *src, size_t n);
 void convert_i64_to_u32(uint32_t *dst, const uint64_t *src, size_t n);
+bool pack_cols(const uint32_t *src, size_t n, uint16_t *lo, uint8_t *hi, int hi_bits);
 }  // namespace mhb
 
 int main() {
@@ -71,6 +72,37 @@ int main() {
         printf("convert_i64_to_u32 mismatch at %zu\n", i);
         return 1;
       }
+    }
+  }
+  // pack_cols: low 16 bits and the bits above (bytes or nibbles) round-trip
+  // every column below 2^(16 + hi_bits); a larger column is reported.
+  for (int t = 0; t < 60; ++t) {
+    const int hb = (t % 2) ? 4 : 8;
+    const size_t lo_off = 2 * (g() % 20);  // even: nibble pairs stay whole
+    const size_t n = (t % 3 == 0) ? (g() % 300) : (1 << 16) + g() % 70000;
+    std::vector<uint32_t> c(n);
+    for (auto &x : c) x = static_cast<uint32_t>(g() % (1ull << (16 + hb)));
+    const bool plant = t % 5 == 4 && n > 0;
+    if (plant) c[g() % n] = 1u << (16 + hb);
+    std::vector<uint16_t> lo(n + 64, 0xAAAA);
+    std::vector<uint8_t> hi(n + 64, 0xAA);
+    const bool ok = mhb::pack_cols(c.data(), n, lo.data() + lo_off, hi.data() + lo_off, hb);
+    if (ok == plant) {
+      printf("pack_cols overflow report wrong (t=%d)\n", t);
+      return 1;
+    }
+    if (plant) continue;
+    for (size_t i = 0; i < n; ++i) {
+      const uint8_t *h = hi.data() + lo_off;
+      const uint32_t hv = hb == 8 ? h[i] : ((h[i / 2] >> ((i & 1) * 4)) & 15u);
+      if ((static_cast<uint32_t>(lo[lo_off + i]) | (hv << 16)) != c[i]) {
+        printf("pack_cols mismatch at %zu (t=%d)\n", i, t);
+        return 1;
+      }
+    }
+    if (lo[lo_off + n] != 0xAAAA) {
+      printf("pack_cols wrote past lo (t=%d)\n", t);
+      return 1;
     }
   }
   printf("ok\n");

@@ -218,6 +218,54 @@ def test_row_block_pipeline(monkeypatch, pinned, block_nnz):
         del keep
 
 
+@pytest.mark.parametrize("pinned", [False, True])
+@pytest.mark.parametrize("dim,no_pack", [((1 << 20) + 123, "0"), (6000, "1")])
+def test_row_block_pipeline_column_packing(monkeypatch, pinned, dim, no_pack):
+    """The pipeline sends columns over the host link as 16 low bits plus 4
+    (dim <= 2^20) or 8 (dim <= 2^24) high bits; byte-wide high parts (dim
+    above 2^20) and the unpacked route (MHCUDA_B200_NO_PACK) give the
+    oracle's hashes too."""
+    rng = np.random.default_rng(dim % 1000 + int(pinned))
+    samples = 32
+    params = gamma_params(rng, dim, samples)
+    m = random_csr(rng, 700, dim, 90, long_rows=[(5, 4000)], empty_frac=0.03)
+    want = O.COracle(*params).hash_csr(m, lnw=device_logf(m.data))
+    with engine_gen(dim, samples, deferred=True) as eng:
+        eng.assign(*params)
+        monkeypatch.setenv("MHCUDA_B200_PIPELINE_MIN_NNZ", "1")
+        monkeypatch.setenv("MHCUDA_B200_BLOCK_NNZ", "7777")
+        monkeypatch.setenv("MHCUDA_B200_NO_PACK", no_pack)
+        data, idx, ip = m.data, m.indices.astype(np.uint32), m.indptr.astype(np.uint32)
+        out = np.full((m.shape[0], samples, 2), 7, np.uint32)
+        keep = []
+        if pinned:
+            (data, t1), (idx, t2), (ip, t3), (out, t4) = (_pinned(data), _pinned(idx), _pinned(ip),
+                                                          _pinned(out))
+            keep = [t1, t2, t3, t4]
+        for _ in range(2):
+            rc = eng.lib.mhcuda_calc(eng.h, data.ctypes.data, idx.ctypes.data, ip.ctypes.data,
+                                     m.shape[0], out.ctypes.data)
+            assert rc == 0
+            np.testing.assert_array_equal(out, want)
+        del keep
+
+
+def test_row_block_pipeline_unpackable_column_is_rejected(monkeypatch):
+    """A column too wide for the packed form (here 2^32 - 1 with dim 500)
+    sends its block unpacked, where the device check rejects it."""
+    rng = np.random.default_rng(78)
+    dim = 500
+    m = random_csr(rng, 400, dim, 30)
+    idx = m.indices.astype(np.uint32).copy()
+    idx[len(idx) // 2] = 0xFFFFFFFF
+    with engine_gen(dim, 64, seed=3) as eng:
+        monkeypatch.setenv("MHCUDA_B200_PIPELINE_MIN_NNZ", "1")
+        monkeypatch.setenv("MHCUDA_B200_BLOCK_NNZ", "1000")
+        rc, _ = eng.calc_raw(m.data, idx, m.indptr)
+        assert rc == 1
+        np.testing.assert_array_equal(eng.calc_csr(m), eng.calc_csr(m))
+
+
 def test_row_block_pipeline_reports_bad_column_in_late_block(monkeypatch):
     rng = np.random.default_rng(77)
     dim = 500
