@@ -39,44 +39,10 @@
 namespace mhb {
 namespace {
 
-#ifndef MHB_L2_HINTS
-#define MHB_L2_HINTS 0
-#endif
-#ifndef MHB_FLOOR_RM
-#define MHB_FLOOR_RM 0
-#endif
-#ifndef MHB_SPAD_TEMPLATES
-#define MHB_SPAD_TEMPLATES 0
-#endif
-
-__device__ __forceinline__ uint64_t l2_policy_evict_first() {
-  uint64_t pol;
-  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
-  return pol;
-}
-__device__ __forceinline__ uint64_t l2_policy_evict_last() {
-  uint64_t pol;
-  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
-  return pol;
-}
-
 template <int SPL>
 struct Lanes {
   float v[SPL];
-  __device__ __forceinline__ void load(const float *__restrict__ p, uint64_t pol) {
-#if MHB_L2_HINTS & 2
-    if constexpr (SPL == 4) {
-      asm("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
-          : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]) : "l"(p), "l"(pol));
-    } else if constexpr (SPL == 2) {
-      asm("ld.global.nc.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;"
-          : "=f"(v[0]), "=f"(v[1]) : "l"(p), "l"(pol));
-    } else {
-      asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v[0]) : "l"(p), "l"(pol));
-    }
-    return;
-#endif
-    (void)pol;
+  __device__ __forceinline__ void load(const float *__restrict__ p) {
     if constexpr (SPL == 4) {
       const float4 x = __ldg(reinterpret_cast<const float4 *>(p));
       v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
@@ -206,11 +172,7 @@ __device__ __forceinline__ void store_final(const HashArgs &a, uint32_t row, uin
   uint32_t *o = a.out + (static_cast<size_t>(row) * a.samples + s0) * 2;
 #pragma unroll
   for (int j = 0; j < SPL; ++j) {
-#if MHB_L2_HINTS & 4
-    if (s0 + j < a.samples) __stcs(reinterpret_cast<uint2 *>(o + 2 * j), resolve(a, st.pos[j], s0 + j));
-#else
     if (s0 + j < a.samples) *reinterpret_cast<uint2 *>(o + 2 * j) = resolve(a, st.pos[j], s0 + j);
-#endif
   }
 }
 
@@ -285,20 +247,11 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, uint32_t 
 // addresses 16-byte aligned, bytes a multiple of 16.  No multicast.
 __device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, uint32_t bytes,
                                               unsigned long long *bar) {
-#if MHB_L2_HINTS & 1
-  // The CSR is read once per launch: evict it from L2 before the parameters.
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
-      " [%0], [%1], %2, [%3], %4;" ::"r"(smem_addr(dst)),
-      "l"(src), "r"(bytes), "r"(smem_addr(bar)), "l"(l2_policy_evict_first())
-      : "memory");
-#else
   asm volatile(
       "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
           smem_addr(dst)),
       "l"(src), "r"(bytes), "r"(smem_addr(bar))
       : "memory");
-#endif
 }
 
 // Positions of a window that arrive by bulk copy: a multiple of 4 (16 bytes
@@ -396,11 +349,10 @@ __device__ __forceinline__ bool finish_window(const HashArgs &a, WarpStage &st, 
 template <int SPL>
 struct Params {
   Lanes<SPL> r, c, b;
-  __device__ __forceinline__ void load(const float *__restrict__ col_base, uint32_t s_pad,
-                                       uint64_t pol) {
-    r.load(col_base, pol);
-    c.load(col_base + s_pad, pol);
-    b.load(col_base + 2 * s_pad, pol);
+  __device__ __forceinline__ void load(const float *__restrict__ col_base, uint32_t s_pad) {
+    r.load(col_base);
+    c.load(col_base + s_pad);
+    b.load(col_base + 2 * s_pad);
   }
 };
 
@@ -471,23 +423,11 @@ __device__ __forceinline__ void eval_all(const Params<SPL> &p, float w, uint32_t
       const F2 va = add2(qa, f2(p.b.v[j], p.b.v[j + 1]));
       float q0, q1;
       split(qa, q0, q1);
-#if MHB_FLOOR_RM
-      // floor(v) = RM(v + 1.5*2^23) - 1.5*2^23 for |v| < 2^22 (the sum lies in
-      // [2^23, 2^24), where rounding toward -inf to an integer is floor); for
-      // larger |v| the margin m >= 16 leaves t undecided.
-      const F2 magic{0x4B4000004B400000ull};  // (1.5*2^23, 1.5*2^23)
-      F2 tt;
-      asm("add.rm.f32x2 %0, %1, %2;" : "=l"(tt.v) : "l"(va.v), "l"(magic.v));
-      tt = sub2(tt, magic);
-      split(tt, t[j], t[j + 1]);
-      const F2 fr = sub2(va, tt);
-#else
       float v0, v1;
       split(va, v0, v1);
       t[j] = floorf(v0);
       t[j + 1] = floorf(v1);
       const F2 fr = sub2(va, f2(t[j], t[j + 1]));
-#endif
       const F2 s = f2(__fadd_rn(fabsf(q0), fabsf(p.b.v[j])),
                       __fadd_rn(fabsf(q1), fabsf(p.b.v[j + 1])));
       const F2 lim = fma2(s, f2(-kTMargin, -kTMargin), f2(0.5f - kTMargin, 0.5f - kTMargin));
@@ -531,7 +471,6 @@ struct WarpCtx {
   PackedStage *pk;  // packed-column landing area (packed kernels only)
   uint32_t parity;  // bit b: phase parity to wait for on buffer b
   uint32_t lane;
-  uint64_t pol;     // L2 policy of the parameter loads
 };
 
 __device__ __forceinline__ void warp_ctx_init(WarpCtx &w, WarpStage *stage_all,
@@ -546,11 +485,6 @@ __device__ __forceinline__ void warp_ctx_init(WarpCtx &w, WarpStage *stage_all,
   }
   __syncwarp();
   w.parity = 0;
-#if MHB_L2_HINTS & 2
-  w.pol = l2_policy_evict_last();
-#else
-  w.pol = 0;
-#endif
 }
 
 // One (chunk c, sample tile) item over the CSR of `a`: finishes the rows
@@ -567,7 +501,6 @@ __device__ __forceinline__ bool hash_item(const HashArgs &a, uint32_t c, uint32_
   WarpStage &stg = *wc.stg;
   PackedStage *pk = wc.pk;
   uint32_t &parity = wc.parity;
-  const uint64_t pol = wc.pol;
   const uint32_t base = a.indptr[0];
   const uint32_t spad = SPAD ? static_cast<uint32_t>(SPAD) : a.s_pad;
   const size_t col_stride = static_cast<size_t>(3) * (SPAD ? static_cast<uint32_t>(SPAD) : a.s_pad);
@@ -647,7 +580,7 @@ __device__ __forceinline__ bool hash_item(const HashArgs &a, uint32_t c, uint32_
       // (finish_window).
       Params<SPL> A, B;
       uint32_t dA = cl[0], dB = 0;
-      A.load(pbase + dA * col_stride, spad, pol);
+      A.load(pbase + dA * col_stride, spad);
       uint32_t i = 0;
       while (i < n) {
         // Row boundaries (warp-uniform): finish rows, start the next owned one.
@@ -668,16 +601,16 @@ __device__ __forceinline__ bool hash_item(const HashArgs &a, uint32_t c, uint32_
         // evaluated, A for i+2 while B is evaluated.
         while (i + 1 < seg) {  // i + 2 <= n
           dB = cl[i + 1];
-          B.load(pbase + dB * col_stride, spad, pol);
+          B.load(pbase + dB * col_stride, spad);
           eval_all<SPL>(A, lw[i], ws + i, active, st);
           dA = cl[i + 2];
-          A.load(pbase + dA * col_stride, spad, pol);
+          A.load(pbase + dA * col_stride, spad);
           eval_all<SPL>(B, lw[i + 1], ws + i + 1, active, st);
           i += 2;
         }
         if (i < seg) {  // i + 1 <= n
           dB = cl[i + 1];
-          B.load(pbase + dB * col_stride, spad, pol);
+          B.load(pbase + dB * col_stride, spad);
           eval_all<SPL>(A, lw[i], ws + i, active, st);
           ++i;
           A = B;
@@ -1010,7 +943,6 @@ using HashFn = void (*)(const HashArgs);
 using BatchFn = void (*)(const BatchArgs);
 
 BatchFn pick_batch(uint32_t spl, uint32_t minb, uint32_t s_pad) {
-#if MHB_SPAD_TEMPLATES
   switch (spl * 100000 + minb * 10000 + s_pad) {
     case 440128: return hash_batch_kernel<4, 4, 128>;
     case 430128: return hash_batch_kernel<4, 3, 128>;
@@ -1019,9 +951,6 @@ BatchFn pick_batch(uint32_t spl, uint32_t minb, uint32_t s_pad) {
     case 240064: return hash_batch_kernel<2, 4, 64>;
     default: break;
   }
-#else
-  (void)s_pad;
-#endif
   switch (spl * 10 + minb) {
     case 44: return hash_batch_kernel<4, 4, 0>;
     case 43: return hash_batch_kernel<4, 3, 0>;
@@ -1035,6 +964,14 @@ BatchFn pick_batch(uint32_t spl, uint32_t minb, uint32_t s_pad) {
 // with s_pad compiled in for the common sample counts.
 HashFn pick_hash(uint32_t spl, uint32_t minb, uint32_t s_pad, bool packed = false) {
   if (packed) {
+    switch (spl * 100000 + minb * 10000 + s_pad) {
+      case 440128: return hash_kernel<4, 4, 128, true>;
+      case 430128: return hash_kernel<4, 3, 128, true>;
+      case 440256: return hash_kernel<4, 4, 256, true>;
+      case 430256: return hash_kernel<4, 3, 256, true>;
+      case 240064: return hash_kernel<2, 4, 64, true>;
+      default: break;
+    }
     switch (spl * 10 + minb) {
       case 44: return hash_kernel<4, 4, 0, true>;
       case 43: return hash_kernel<4, 3, 0, true>;
@@ -1043,7 +980,6 @@ HashFn pick_hash(uint32_t spl, uint32_t minb, uint32_t s_pad, bool packed = fals
       default: return nullptr;
     }
   }
-#if MHB_SPAD_TEMPLATES
   switch (spl * 100000 + minb * 10000 + s_pad) {
     case 440128: return hash_kernel<4, 4, 128, false>;
     case 430128: return hash_kernel<4, 3, 128, false>;
@@ -1052,9 +988,6 @@ HashFn pick_hash(uint32_t spl, uint32_t minb, uint32_t s_pad, bool packed = fals
     case 240064: return hash_kernel<2, 4, 64, false>;
     default: break;
   }
-#else
-  (void)s_pad;
-#endif
   switch (spl * 10 + minb) {
     case 44: return hash_kernel<4, 4, 0, false>;
     case 43: return hash_kernel<4, 3, 0, false>;

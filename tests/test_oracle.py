@@ -160,3 +160,13 @@ def test_golden_vectors():
         np.testing.assert_array_equal(out[mask], ref[mask], err_msg=os.path.basename(f))
         # Cells with no selectable entry are undefined in the reference.
         assert mask.mean() > 0.5
+
+
+def test_every_recorded_golden_case_is_committed():
+    """Each case tests/golden/make_golden.py records from the reference build
+    has its file here, so test_golden_vectors pins all of them."""
+    import re
+    src = open(os.path.join(GOLDEN, "make_golden.py")).read()
+    names = set(re.findall(r'record\(args\.out, "([a-z0-9_]+)"', src))
+    have = {os.path.basename(f)[:-4] for f in glob.glob(os.path.join(GOLDEN, "*.npz"))}
+    assert names and names <= have, sorted(names - have)
