@@ -143,6 +143,20 @@ enum MHCUDAResult mhcuda_calc_batch(
     const uint32_t *const *rows, const uint32_t *lengths,
     uint32_t *const *outputs);
 
+/* Page-locks (registers) `bytes` of the caller's host memory at `ptr` for the
+ * copy engines of every device (cudaHostRegisterPortable; the context of the
+ * device selected like mhcuda_init's `devices` mask does the registering),
+ * or releases such a registration.  mhcuda_calc then copies a CSR held in
+ * registered memory straight to the device, with no staging copy on host
+ * threads.  Registering runs at about the speed of one pageable copy of the
+ * same bytes, so it pays for data hashed more than once (several generators,
+ * repeated row-block passes); the Python module's minhash_cuda_pin uses it.
+ * Returns mhcudaInvalidArguments for a range that is already registered.
+ * No counterpart in the reference (its calls copy from pageable memory,
+ * minhashcuda.cc:385-455). */
+enum MHCUDAResult mhcuda_host_register(uint32_t devices, const void *ptr, uint64_t bytes);
+enum MHCUDAResult mhcuda_host_unregister(uint32_t devices, const void *ptr);
+
 /* Test hook: evaluates the device logf (the one the hash kernel applies to
  * every weight) on n host floats, on the device selected like mhcuda_init's
  * `devices` mask.  No counterpart in the reference. */

@@ -74,6 +74,8 @@ SIGNATURES = {
     "mhcuda_calc_batch": (_RES, [_P, _U32, _P, _P, _P, _P, _P]),
     "mhcuda_calc_batch_device": (_RES, [_P, _U32, _P, _P, _P, _P, _P, _P]),
     "mhcuda_debug_device_logf": (_RES, [_U32, _P, _P, ctypes.c_uint64]),
+    "mhcuda_host_register": (_RES, [_U32, _P, ctypes.c_uint64]),
+    "mhcuda_host_unregister": (_RES, [_U32, _P]),
     "mhcuda_lsh_bands": (_RES, [_P, _P, _U32, _U32, _P, _P]),
     "mhcuda_jaccard": (_RES, [_P, _P, _U32, _P, ctypes.c_uint64, _P, _P]),
     "mhcuda_server_start": (_P, [_U32, ctypes.c_uint64, _U32, ctypes.c_int,

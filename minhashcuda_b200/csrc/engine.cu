@@ -313,7 +313,8 @@ HashPlan make_plan(const Gen *gen, uint64_t nnz, uint64_t rows, const TuneChoice
   }
   const uint32_t tile_w = 32u * p.spl;
   p.ntiles = (s_pad + tile_w - 1) / tile_w;
-  const int bps = mhb::hash_blocks_per_sm(p.spl, p.minb, s_pad);
+  p.ring = static_cast<uint32_t>(std::max(0, env_int("MHCUDA_B200_RING", 0)));
+  const int bps = mhb::hash_blocks_per_sm(p.spl, p.minb, s_pad, p.ring);
   const uint64_t resident_warps =
       static_cast<uint64_t>(gen->sm_count) * bps * (mhb::kHashBlock / 32);
   const int waves = std::max(
@@ -559,12 +560,18 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
   const bool pin_in = in.native() && is_pinned(in.weights) && is_pinned(in.cols) &&
                       is_pinned(rows);
   const bool pin_out = is_pinned(output);
-  // 32-bit columns cross the host link packed when dim allows it: 16 low
-  // bits plus 4 (dim <= 2^20) or 8 (dim <= 2^24) high bits, 6.5 or 7 bytes
-  // per entry with the weight instead of 8 (the link bounds this path).
-  const int pack_bits = (in.cols64 == 0 && env_int("MHCUDA_B200_NO_PACK", 0) == 0)
-                            ? (gen->dim <= (1u << 20) ? 4 : (gen->dim <= (1u << 24) ? 8 : 0))
-                            : 0;
+  // Pageable 32-bit columns are staged by host threads anyway: they are
+  // packed on the way (16 low bits plus 4 high bits when dim <= 2^20, 8 when
+  // dim <= 2^24), which writes 2.5-3 instead of 4 bytes per entry to the
+  // staging and sends 6.5-7 instead of 8 bytes per entry over the link.
+  // Page-locked columns are copied by the DMA engine straight from the
+  // caller: packing them would add host memory traffic the copy does not
+  // have (measured: 486 vs 448 ms per step on 2.8e9 entries), so they cross
+  // as they are.
+  const int pack_bits =
+      (in.cols64 == 0 && !pin_in && env_int("MHCUDA_B200_NO_PACK", 0) == 0)
+          ? (gen->dim <= (1u << 20) ? 4 : (gen->dim <= (1u << 24) ? 8 : 0))
+          : 0;
   // Page-locked inputs copy straight from the caller: large blocks.  Pageable
   // ones go through pinned staging, which is cheaper to allocate (and
   // re-fill) in smaller blocks.
@@ -1682,6 +1689,34 @@ enum MHCUDAResult mhcuda_calc_batch(const MinhashCudaGenerator *gen, uint32_t co
     return r;
   }
   return read_status(gen, st);
+}
+
+enum MHCUDAResult mhcuda_host_register(uint32_t devices, const void *ptr, uint64_t bytes) {
+  if (!ptr || bytes == 0) return mhcudaInvalidArguments;
+  const int dev = pick_device(devices);
+  if (dev < 0) return mhcudaNoSuchDevice;
+  mhb::DeviceGuard on_device(dev);
+  if (!on_device.ok()) return mhcudaNoSuchDevice;
+  const cudaError_t e =
+      cudaHostRegister(const_cast<void *>(ptr), static_cast<size_t>(bytes), cudaHostRegisterPortable);
+  if (e == cudaSuccess) return mhcudaSuccess;
+  cudaGetLastError();
+  return e == cudaErrorHostMemoryAlreadyRegistered || e == cudaErrorInvalidValue
+             ? mhcudaInvalidArguments
+             : mhcudaMemoryAllocationFailure;
+}
+
+enum MHCUDAResult mhcuda_host_unregister(uint32_t devices, const void *ptr) {
+  if (!ptr) return mhcudaInvalidArguments;
+  const int dev = pick_device(devices);
+  if (dev < 0) return mhcudaNoSuchDevice;
+  mhb::DeviceGuard on_device(dev);
+  if (!on_device.ok()) return mhcudaNoSuchDevice;
+  if (cudaHostUnregister(const_cast<void *>(ptr)) != cudaSuccess) {
+    cudaGetLastError();
+    return mhcudaInvalidArguments;
+  }
+  return mhcudaSuccess;
 }
 
 enum MHCUDAResult mhcuda_debug_device_logf(uint32_t devices, const float *in, float *out,

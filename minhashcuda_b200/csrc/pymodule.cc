@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <ctime>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "minhashcuda.h"
@@ -337,6 +338,91 @@ PyObject *py_calc_batch(PyObject *, PyObject *args) {
   return result.release();
 }
 
+// Matrices page-locked by minhash_cuda_pin: handle -> the registered arrays
+// (held, so their memory stays valid while registered) and the device mask.
+struct Pinned {
+  std::vector<PyObject *> arrays;
+  uint32_t devices = 0;
+};
+std::unordered_map<unsigned long long, Pinned> g_pinned;
+unsigned long long g_next_pin = 1;
+
+void release_pinned(Pinned &p) {
+  for (PyObject *a : p.arrays) {
+    const void *ptr = PyArray_DATA(reinterpret_cast<PyArrayObject *>(a));
+    Py_BEGIN_ALLOW_THREADS
+    mhcuda_host_unregister(p.devices, ptr);
+    Py_END_ALLOW_THREADS
+    Py_DECREF(a);
+  }
+  p.arrays.clear();
+}
+
+// minhash_cuda_pin(matrix, devices=0) -> handle.  Page-locks the float32
+// data and 32-bit indices/indptr of a CSR matrix in place, so that
+// minhash_cuda_calc copies them to the device directly -- the case of a large
+// matrix hashed in several row_start/row_finish blocks, several times or by
+// several generators.  The arrays are kept alive until minhash_cuda_unpin.
+PyObject *py_pin(PyObject *, PyObject *args, PyObject *kwargs) {
+  static const char *kw[] = {"matrix", "devices", nullptr};
+  PyObject *m = nullptr;
+  unsigned int devices = 0;
+  if (!PyArg_ParseTupleAndKeywords(args, kwargs, "O|I", const_cast<char **>(kw), &m, &devices))
+    return nullptr;
+  Csr v;
+  if (!csr_view(m, &v, /*wide=*/true)) return nullptr;
+  const bool native = v.wtype == mhcudaFloat32 &&
+                      (v.ctype == mhcudaUInt32 || v.ctype == mhcudaInt32) &&
+                      (v.rtype == mhcudaUInt32 || v.rtype == mhcudaInt32);
+  const char *attrs[3] = {"data", "indices", "indptr"};
+  PyArrayObject *views[3] = {v.data.arr(), v.indices.arr(), v.indptr.arr()};
+  Pinned p;
+  p.devices = devices;
+  for (int i = 0; i < 3; ++i) {
+    // Only the matrix's own arrays: pinning a converted copy would not
+    // reach the buffers the calls read.
+    Ref own(PyObject_GetAttrString(m, attrs[i]));
+    if (!native || !own || !PyArray_Check(own.get()) ||
+        PyArray_DATA(reinterpret_cast<PyArrayObject *>(own.get())) != PyArray_DATA(views[i])) {
+      release_pinned(p);
+      PyErr_SetString(PyExc_ValueError,
+                      "minhash_cuda_pin needs contiguous float32 data and 32-bit indices and "
+                      "indptr");
+      return nullptr;
+    }
+    const void *ptr = PyArray_DATA(views[i]);
+    const uint64_t bytes = static_cast<uint64_t>(PyArray_NBYTES(views[i]));
+    if (bytes == 0) continue;
+    MHCUDAResult r;
+    Py_BEGIN_ALLOW_THREADS
+    r = mhcuda_host_register(devices, ptr, bytes);
+    Py_END_ALLOW_THREADS
+    if (!check(r, "minhash_cuda_pin")) {
+      release_pinned(p);
+      return nullptr;
+    }
+    Py_INCREF(reinterpret_cast<PyObject *>(views[i]));
+    p.arrays.push_back(reinterpret_cast<PyObject *>(views[i]));
+  }
+  const unsigned long long h = g_next_pin++;
+  g_pinned.emplace(h, std::move(p));
+  return PyLong_FromUnsignedLongLong(h);
+}
+
+// minhash_cuda_unpin(handle): releases a minhash_cuda_pin registration.
+PyObject *py_unpin(PyObject *, PyObject *args) {
+  unsigned long long h = 0;
+  if (!PyArg_ParseTuple(args, "K", &h)) return nullptr;
+  auto it = g_pinned.find(h);
+  if (it == g_pinned.end()) {
+    PyErr_SetString(PyExc_ValueError, "minhash_cuda_unpin: unknown handle");
+    return nullptr;
+  }
+  release_pinned(it->second);
+  g_pinned.erase(it);
+  Py_RETURN_NONE;
+}
+
 PyObject *py_fini(PyObject *, PyObject *args) {
   unsigned long long g = 0;
   if (!PyArg_ParseTuple(args, "K", &g)) return nullptr;
@@ -361,6 +447,10 @@ PyMethodDef kMethods[] = {
     {"minhash_cuda_calc_batch", py_calc_batch, METH_VARARGS,
      "Calculates Weighted Minhashes of several CSR matrices in one device pass."},
     {"minhash_cuda_fini", py_fini, METH_VARARGS, "Disposes Weighted Minhash internal state on GPU."},
+    {"minhash_cuda_pin", reinterpret_cast<PyCFunction>(reinterpret_cast<void (*)(void)>(py_pin)),
+     METH_VARARGS | METH_KEYWORDS,
+     "Page-locks a CSR matrix's arrays in place for direct copies; returns a handle."},
+    {"minhash_cuda_unpin", py_unpin, METH_VARARGS, "Releases a minhash_cuda_pin handle."},
     {nullptr, nullptr, 0, nullptr}};
 
 PyModuleDef kModule = {PyModuleDef_HEAD_INIT, "libMHCUDA",

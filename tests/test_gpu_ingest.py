@@ -124,3 +124,40 @@ def test_typed_rejects_decreasing_wide_offsets():
         rc, _ = _typed(gen, m.data.astype(np.float64), mb.FLOAT64, m.indices.astype(np.int64),
                        mb.INT64, rows, mb.INT64, m.shape[0], 32)
         assert rc == mb.INVALID_ARGUMENTS
+
+
+@pytest.mark.gpu
+def test_pinned_matrix_streams_row_blocks(monkeypatch):
+    """minhash_cuda_pin page-locks a matrix's own arrays; row_start/row_finish
+    blocks of it then go to the device straight from them (the pipeline sees
+    page-locked input) and equal the unpinned calls and the oracle."""
+    import oracle as O
+    from wmh_testlib import device_logf, gamma_params
+    rng = np.random.default_rng(57)
+    dim, samples = 4000, 128
+    m = random_csr(rng, 3000, dim, 60, empty_frac=0.02, long_rows=[(11, 3000)])
+    m.indices = m.indices.astype(np.int32)
+    m.indptr = m.indptr.astype(np.int32)
+    params = gamma_params(rng, dim, samples)
+    want = O.COracle(*params).hash_csr(m, lnw=device_logf(m.data))
+    gen = L.minhash_cuda_init(dim, samples, deferred=True)
+    try:
+        L.minhash_cuda_assign_vars(gen, *params)
+        monkeypatch.setenv("MHCUDA_B200_PIPELINE_MIN_NNZ", "1")
+        monkeypatch.setenv("MHCUDA_B200_BLOCK_NNZ", "5000")
+        h = L.minhash_cuda_pin(m)
+        try:
+            assert mb.capi().mhcuda_host_register(0, m.data.ctypes.data, m.data.nbytes) == \
+                mb.INVALID_ARGUMENTS  # already registered
+            for r0, r1 in ((0, 700), (700, 2500), (2500, 3000)):
+                np.testing.assert_array_equal(
+                    L.minhash_cuda_calc(gen, m, row_start=r0, row_finish=r1), want[r0:r1])
+        finally:
+            L.minhash_cuda_unpin(h)
+        with pytest.raises(ValueError):
+            L.minhash_cuda_unpin(h)
+        np.testing.assert_array_equal(L.minhash_cuda_calc(gen, m), want)
+        with pytest.raises(ValueError):
+            L.minhash_cuda_pin(_wide(m))  # float64 / int64: would not be read in place
+    finally:
+        L.minhash_cuda_fini(gen)
