@@ -313,8 +313,7 @@ HashPlan make_plan(const Gen *gen, uint64_t nnz, uint64_t rows, const TuneChoice
   }
   const uint32_t tile_w = 32u * p.spl;
   p.ntiles = (s_pad + tile_w - 1) / tile_w;
-  p.ring = static_cast<uint32_t>(std::max(0, env_int("MHCUDA_B200_RING", 0)));
-  const int bps = mhb::hash_blocks_per_sm(p.spl, p.minb, s_pad, p.ring);
+  const int bps = mhb::hash_blocks_per_sm(p.spl, p.minb, s_pad);
   const uint64_t resident_warps =
       static_cast<uint64_t>(gen->sm_count) * bps * (mhb::kHashBlock / 32);
   const int waves = std::max(

@@ -346,53 +346,9 @@ __device__ __forceinline__ bool finish_window(const HashArgs &a, WarpStage &st, 
   return true;
 }
 
-// Parameter ring (RING > 0 positions deep, per warp): lane l stages the
-// r / ln_c / beta vectors of its samples for the next RING positions into
-// v[slot][0..2][l*SPL ..] with cp.async, so the gathers of several positions
-// are in flight without holding registers; each lane reads back only what it
-// copied itself.
-template <int SPL, int RING>
-struct alignas(16) ParamRing {
-  float v[RING > 0 ? RING : 1][3][32 * SPL];
-};
-
-template <int BYTES>
-__device__ __forceinline__ void cp_async_ca(uint32_t dst, const void *src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(dst), "l"(src), "n"(BYTES)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() {
-  asm volatile("cp.async.commit_group;" ::: "memory");
-}
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
-template <int SPL, int RING>
-__device__ __forceinline__ void ring_issue(ParamRing<SPL, RING> &rg, uint32_t slot,
-                                           const float *__restrict__ col_base, uint32_t s_pad,
-                                           uint32_t lane) {
-  const uint32_t dst = static_cast<uint32_t>(__cvta_generic_to_shared(&rg.v[slot][0][lane * SPL]));
-  constexpr uint32_t kPart = 32u * SPL * sizeof(float);
-  cp_async_ca<4 * SPL>(dst, col_base);
-  cp_async_ca<4 * SPL>(dst + kPart, col_base + s_pad);
-  cp_async_ca<4 * SPL>(dst + 2 * kPart, col_base + 2 * s_pad);
-}
-
 template <int SPL>
 struct Params {
   Lanes<SPL> r, c, b;
-  template <int RING>
-  __device__ __forceinline__ void lds(const ParamRing<SPL, RING> &rg, uint32_t slot,
-                                      uint32_t lane) {
-#pragma unroll
-    for (int j = 0; j < SPL; ++j) {
-      r.v[j] = rg.v[slot][0][lane * SPL + j];
-      c.v[j] = rg.v[slot][1][lane * SPL + j];
-      b.v[j] = rg.v[slot][2][lane * SPL + j];
-    }
-  }
   __device__ __forceinline__ void load(const float *__restrict__ col_base, uint32_t s_pad) {
     r.load(col_base);
     c.load(col_base + s_pad);
@@ -513,18 +469,15 @@ __device__ __forceinline__ void eval_all(const Params<SPL> &p, float w, uint32_t
 struct WarpCtx {
   WarpStage *stg;
   PackedStage *pk;  // packed-column landing area (packed kernels only)
-  void *ring;       // ParamRing of this warp (ring kernels only)
   uint32_t parity;  // bit b: phase parity to wait for on buffer b
   uint32_t lane;
 };
 
 __device__ __forceinline__ void warp_ctx_init(WarpCtx &w, WarpStage *stage_all,
-                                              PackedStage *packed_all = nullptr,
-                                              void *ring = nullptr) {
+                                              PackedStage *packed_all = nullptr) {
   w.lane = threadIdx.x & 31u;
   w.stg = &stage_all[threadIdx.x >> 5];
   w.pk = packed_all ? &packed_all[threadIdx.x >> 5] : nullptr;
-  w.ring = ring;
   if (w.lane == 0) {
     mbar_init(&w.stg->bar[0], 1);
     mbar_init(&w.stg->bar[1], 1);
@@ -541,7 +494,7 @@ __device__ __forceinline__ void warp_ctx_init(WarpCtx &w, WarpStage *stage_all,
 // SPAD: the generator's s_pad when it is known at compile time (0: read it
 // from the arguments), which turns the parameter-block addressing into one
 // wide multiply-add and immediate load offsets.
-template <int SPL, int SPAD, bool PACKED, int RING = 0>
+template <int SPL, int SPAD, bool PACKED>
 __device__ __forceinline__ bool hash_item(const HashArgs &a, uint32_t c, uint32_t tile,
                                           WarpCtx &wc) {
   const uint32_t lane = wc.lane;
@@ -602,7 +555,6 @@ __device__ __forceinline__ bool hash_item(const HashArgs &a, uint32_t c, uint32_
     // Error exits wait (bounded) for the windows still in flight into this
     // warp's staging buffers before leaving: windows [from, min(from+2, nwin)).
     auto drain = [&](uint32_t from) {
-      if constexpr (RING > 0) cp_async_wait<0>();
       for (uint32_t kk = from; kk < nwin && kk < from + 2; ++kk) {
         const uint32_t bb = kk & 1u;
         for (uint32_t spins = 0; !mbar_try_wait(&stg.bar[bb], (parity >> bb) & 1u);)
@@ -626,46 +578,6 @@ __device__ __forceinline__ bool hash_item(const HashArgs &a, uint32_t c, uint32_
 
       // Columns in the window are < dim, and slot n holds column 0
       // (finish_window).
-      if constexpr (RING > 0) {
-        ParamRing<SPL, RING> &rg = *static_cast<ParamRing<SPL, RING> *>(wc.ring);
-#pragma unroll
-        for (int d = 0; d < RING; ++d) {
-          if (static_cast<uint32_t>(d) < n) ring_issue(rg, d, pbase + cl[d] * col_stride, spad, lane);
-          cp_async_commit();
-        }
-        uint32_t i = 0, slot = 0;
-        while (i < n) {
-          while (ws + i >= row_end) {
-            flush();
-            if (r_next >= r_stop) {  // only reachable with inconsistent offsets
-              if (lane == 0) atomicOr(a.status, kStatusBadIndptr);
-              drain(k + 1);
-              return false;
-            }
-            row = r_next++;
-            row_end = a.indptr[row + 1] - base;
-            head = false;
-            st.reset();
-          }
-          const uint32_t seg = min(row_end - ws, n);
-          for (; i < seg; ++i) {
-            cp_async_wait<RING - 1>();
-            Params<SPL> P;
-            P.lds(rg, slot, lane);
-            eval_all<SPL>(P, lw[i], ws + i, active, st);
-            // The slot's values are in registers and used: refill it.
-            if (i + RING < n) ring_issue(rg, slot, pbase + cl[i + RING] * col_stride, spad, lane);
-            cp_async_commit();
-            slot = slot + 1 == RING ? 0 : slot + 1;
-          }
-        }
-        cp_async_wait<0>();
-        if (k + 2 < nwin) {
-          const uint32_t ws2 = ws + 2 * kWin;
-          issue_window<PACKED>(a, stg, pk, b, ws2, min(kWin, ce - ws2), bulk_ok, lane);
-        }
-        continue;
-      }
       Params<SPL> A, B;
       uint32_t dA = cl[0], dB = 0;
       A.load(pbase + dA * col_stride, spad);
@@ -725,7 +637,7 @@ __device__ __forceinline__ bool hash_item(const HashArgs &a, uint32_t c, uint32_
 }
 
 // PACKED: the columns arrive as cols_lo/cols_hi (HashArgs::col_hi_bits).
-template <int SPL, int MINB, int SPAD, bool PACKED, int RING = 0>
+template <int SPL, int MINB, int SPAD, bool PACKED>
 __global__ void __launch_bounds__(kHashBlock, MINB) hash_kernel(const HashArgs a) {
   __shared__ WarpStage stage_all[kHashBlock / 32];
   PackedStage *packed_all = nullptr;
@@ -733,21 +645,15 @@ __global__ void __launch_bounds__(kHashBlock, MINB) hash_kernel(const HashArgs a
     __shared__ PackedStage packed_stage[kHashBlock / 32];
     packed_all = packed_stage;
   }
-  void *ring = nullptr;
-  if constexpr (RING > 0) {
-    // Dynamic shared memory: kHashBlock / 32 rings (ring_bytes()).
-    extern __shared__ __align__(16) unsigned char ring_smem[];
-    ring = ring_smem + (threadIdx.x >> 5) * sizeof(ParamRing<SPL, RING>);
-  }
   if (*a.status & kStatusBadIndptr) return;
   WarpCtx wc;
-  warp_ctx_init(wc, stage_all, packed_all, ring);
+  warp_ctx_init(wc, stage_all, packed_all);
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
   const uint32_t items = a.nchunks * a.ntiles;
   for (uint32_t item = gw; item < items; item += nw) {
     const uint32_t c = item / a.ntiles;
-    if (!hash_item<SPL, SPAD, PACKED, RING>(a, c, item - c * a.ntiles, wc)) return;
+    if (!hash_item<SPL, SPAD, PACKED>(a, c, item - c * a.ntiles, wc)) return;
   }
 }
 
@@ -1056,18 +962,7 @@ BatchFn pick_batch(uint32_t spl, uint32_t minb, uint32_t s_pad) {
 
 // Instantiated (samples per lane, minimum resident blocks per SM) variants,
 // with s_pad compiled in for the common sample counts.
-HashFn pick_hash(uint32_t spl, uint32_t minb, uint32_t s_pad, bool packed = false,
-                 uint32_t ring = 0) {
-  if (ring && !packed && spl == 4 && s_pad == 128) {
-    switch (minb * 10 + ring) {
-      case 32: return hash_kernel<4, 3, 128, false, 2>;
-      case 33: return hash_kernel<4, 3, 128, false, 3>;
-      case 34: return hash_kernel<4, 3, 128, false, 4>;
-      case 42: return hash_kernel<4, 4, 128, false, 2>;
-      case 43: return hash_kernel<4, 4, 128, false, 3>;
-      default: break;
-    }
-  }
+HashFn pick_hash(uint32_t spl, uint32_t minb, uint32_t s_pad, bool packed = false) {
   if (packed) {
     switch (spl * 100000 + minb * 10000 + s_pad) {
       case 440128: return hash_kernel<4, 4, 128, true>;
@@ -1104,26 +999,10 @@ HashFn pick_hash(uint32_t spl, uint32_t minb, uint32_t s_pad, bool packed = fals
 
 }  // namespace
 
-// Dynamic shared memory of a ring kernel: one ParamRing per warp.
-size_t ring_bytes(uint32_t spl, uint32_t ring) {
-  return ring ? static_cast<size_t>(kHashBlock / 32) * ring * 3 * 32 * spl * sizeof(float) : 0;
-}
-
-// Ring kernels need more than the default 48 KB of dynamic shared memory.
-cudaError_t prepare_ring(HashFn fn, size_t bytes) {
-  if (!bytes) return cudaSuccess;
-  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              static_cast<int>(bytes));
-}
-
 cudaError_t launch_hash(const HashArgs &a, const HashPlan &plan, cudaStream_t stream) {
-  const HashFn fn = pick_hash(plan.spl, plan.minb, a.s_pad, a.col_hi_bits != 0, plan.ring);
+  const HashFn fn = pick_hash(plan.spl, plan.minb, a.s_pad, a.col_hi_bits != 0);
   if (!fn) return cudaErrorInvalidValue;
-  const bool ring = plan.ring && pick_hash(plan.spl, plan.minb, a.s_pad, a.col_hi_bits != 0, 0) != fn;
-  const size_t dyn = ring ? ring_bytes(plan.spl, plan.ring) : 0;
-  const cudaError_t e = prepare_ring(fn, dyn);
-  if (e != cudaSuccess) return e;
-  fn<<<plan.grid, kHashBlock, dyn, stream>>>(a);
+  fn<<<plan.grid, kHashBlock, 0, stream>>>(a);
   return cudaGetLastError();
 }
 
@@ -1151,12 +1030,10 @@ cudaError_t launch_batch(const BatchArgs &b, const HashPlan &plan, uint32_t plan
   return cudaGetLastError();
 }
 
-int hash_blocks_per_sm(uint32_t spl, uint32_t minb, uint32_t s_pad, uint32_t ring) {
-  const HashFn fn = pick_hash(spl, minb, s_pad, false, ring);
-  const size_t dyn = fn != pick_hash(spl, minb, s_pad, false, 0) ? ring_bytes(spl, ring) : 0;
+int hash_blocks_per_sm(uint32_t spl, uint32_t minb, uint32_t s_pad) {
+  const HashFn fn = pick_hash(spl, minb, s_pad);
   int n = 0;
-  if (!fn || prepare_ring(fn, dyn) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kHashBlock, dyn) != cudaSuccess) {
+  if (!fn || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kHashBlock, 0) != cudaSuccess) {
     cudaGetLastError();
     return 1;
   }

@@ -123,6 +123,11 @@ struct MinhashCudaServer_ {
   size_t scratch_unit = 0;  // scratch = chunk_row (1 unit) | part_ln (4) | part_kt (8)
   uint64_t max_unit_evals = 128ull << 20;   // nnz*samples: high-priority batch limit
   uint64_t max_batch_evals = 512ull << 20;  // nnz*samples of one lane batch
+  // Warp items per resident warp a batch is cut into at least (small ones:
+  // `min_items_high`, large ones: `min_items_low`).  Finer items for large
+  // batches retire their blocks sooner, so a small batch's blocks find SMs
+  // sooner.
+  uint32_t min_items_high = 2, min_items_low = 2;
   uint32_t max_low_inflight = 6;            // low-priority batches out at once (lanes - 2)
   uint64_t zero_copy_max_bytes = ~0ull;     // CSR bytes of a batch read from mapped memory
   uint32_t low_inflight = 0;
@@ -299,7 +304,8 @@ MHCUDAResult MinhashCudaServer_::run_units(Lane &lane, const std::vector<Unit> &
   // Batches are small next to a plain call: at least two waves of warp items
   // even when rows are long (the plain plan keeps a few rows per chunk);
   // several lanes' launches overlap, so two are enough.
-  mhb::HashPlan plan = mhb::plan_for_generator(units.front().req->gen, N, R, 2);
+  mhb::HashPlan plan = mhb::plan_for_generator(units.front().req->gen, N, R,
+                                               high ? min_items_high : min_items_low);
   const int bps = mhb::hash_blocks_per_sm(plan.spl, plan.minb, s_pad);
   // Keep the chunk table and partials inside the lane's fixed scratch:
   // nchunks*4 <= unit, 2*nchunks*s_pad*4 <= 4*unit, 2*nchunks*s_pad*8 <= 8*unit.
@@ -586,6 +592,10 @@ MinhashCudaServer *mhcuda_server_start(uint32_t devices, uint64_t hbm_budget_byt
   srv->max_batch_evals = env_u64("MHCUDA_B200_SERVER_BATCH_EVALS", srv->max_batch_evals);
   srv->zero_copy_max_bytes = env_u64("MHCUDA_B200_SERVER_ZERO_COPY_MAX_BYTES", ~0ull);
   if (const char *tp = getenv("MHCUDA_B200_SERVER_TRACE")) srv->trace_path = tp;
+  srv->min_items_high =
+      static_cast<uint32_t>(env_u64("MHCUDA_B200_SERVER_MIN_ITEMS_HIGH", srv->min_items_high));
+  srv->min_items_low =
+      static_cast<uint32_t>(env_u64("MHCUDA_B200_SERVER_MIN_ITEMS_LOW", srv->min_items_low));
   srv->max_low_inflight = static_cast<uint32_t>(std::min<uint64_t>(
       lanes, env_u64("MHCUDA_B200_SERVER_LOW_INFLIGHT", lanes > 2 ? lanes - 2 : 1)));
   cudaDeviceGetAttribute(&srv->sm_count, cudaDevAttrMultiProcessorCount, dev);

@@ -44,7 +44,6 @@ struct HashPlan {
   uint32_t minb;     // kernel variant: minimum resident blocks per SM (4, or 3 for spl 4)
   uint32_t ntiles;   // sample tiles of 32*spl samples
   uint32_t grid;     // persistent grid (blocks of kHashBlock threads)
-  uint32_t ring;     // parameter prefetch ring depth (0: two register sets)
 };
 
 constexpr int kHashBlock = 256;
@@ -123,7 +122,7 @@ cudaError_t launch_batch(const BatchArgs &b, const HashPlan &plan, uint32_t plan
                          cudaStream_t stream);
 // Blocks per SM the hash kernel variant launched for (samples per lane,
 // register budget, s_pad) reaches, and its registers per thread.
-int hash_blocks_per_sm(uint32_t spl, uint32_t minb, uint32_t s_pad, uint32_t ring = 0);
+int hash_blocks_per_sm(uint32_t spl, uint32_t minb, uint32_t s_pad);
 size_t hash_kernel_registers(uint32_t spl, uint32_t minb, uint32_t s_pad);
 
 // Parameter kernels (param_kernels.cu).
