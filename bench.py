@@ -143,14 +143,19 @@ def kernel_source_sha16():
         return hashlib.sha256(f.read()).hexdigest()[:16]
 
 
-def kernel_profile():
-    """Counters ncu measured for the hash kernel on a 20,000-row case of the
-    large workload (profiles/hash_kernel_traffic.json), and whether they were
-    taken on the kernel source this run built."""
+def kernel_profile(variant):
+    """Counters ncu measured for the hash kernel variant `variant` (e.g.
+    "spl4_minb3") on a 20,000-row case of the large workload
+    (profiles/hash_kernel_traffic.json), and whether they were taken on the
+    kernel source this run built."""
     if not os.path.exists(PROFILE_JSON):
         return None, False
     d = json.load(open(PROFILE_JSON))
-    return d, d.get("source_sha16") == kernel_source_sha16()
+    v = d.get("variants", {}).get(variant)
+    if v is None:
+        return None, False
+    v = dict(v, captured_case=d.get("captured_case"), variant=variant)
+    return v, d.get("source_sha16") == kernel_source_sha16()
 
 
 def digest(a):
@@ -193,6 +198,7 @@ def hash_roofline(nnz, R, S, kernel_ms, sm_mhz, peak, peak_kind, profile, profil
                              "frac": fp / issue_peak, "ops_per_eval": 8}
     out["profile"] = {"source": os.path.relpath(PROFILE_JSON, ROOT),
                       "case": profile.get("captured_case") if profile else None,
+                      "variant": profile.get("variant") if profile else None,
                       "matches_built_kernel": profile_current}
     if cands:
         bound = max(cands, key=lambda k: cands[k]["frac"])
@@ -1157,7 +1163,12 @@ def main():
 
     hash_ms_launch = hash_ms.value / max(1, launches.value)
     peak, peak_kind = measured_peaks()
-    prof, prof_current = kernel_profile() if w.name == "large" else (None, False)
+    if tuned:
+        variant = f"spl{tuned['samples_per_lane']}_minb{tuned['min_blocks_per_sm']}"
+    else:
+        variant = f"spl{os.environ.get('MHCUDA_B200_SPL', '4')}_minb" \
+                  f"{os.environ.get('MHCUDA_B200_MINB', '4')}"
+    prof, prof_current = kernel_profile(variant) if w.name == "large" else (None, False)
     roofline = hash_roofline(nnz, R, S, hash_ms_launch, clocks.get("sm_mhz"), peak, peak_kind,
                              prof, prof_current)
 
