@@ -1011,7 +1011,7 @@ def run_extras(args, rank, world, local, lib, peak, peak_kind):
             ["value", "unit", "config", "rows_per_s", "seconds_total", "pass_seconds",
              "device_resident", "streamed_equals_device_path", "e2e"]),
         "serving": lambda: summary(
-            run_serving(args, rank, world, local, emit=False, seconds=3.0),
+            run_serving(args, rank, world, local, emit=False, seconds=5.0),
             ["metric", "value", "unit", "config", "saturated_evals_per_s", "levels",
              "bit_exact_served_vs_alone"]),
     }

@@ -41,7 +41,8 @@ def test_hash_roofline_picks_the_binding_resource():
     names the one closest to its peak; the algorithmic-byte rate is kept
     beside them."""
     b = _bench()
-    prof = {"dram_bytes_per_eval": 4.0, "thread_inst_per_eval": 20.0, "captured_case": "x"}
+    prof = {"dram_bytes_per_eval": 4.0, "thread_inst_per_eval": 20.0, "captured_case": "x",
+            "variant": "spl4_minb3"}
     nnz, R, S = 1_000_000_000, 1_000_000, 128
     evals = nnz * S
     t_ms = 200.0
@@ -71,3 +72,17 @@ def test_small_config_matrix_matches_the_oracle_restatement():
     _, m = O.reference_small_matrix(1)
     assert np.array_equal(ip, m.indptr) and np.array_equal(cols, m.indices)
     assert np.array_equal(w, m.data)
+
+
+def test_kernel_profile_matches_the_built_source():
+    """The committed ncu counters name the kernel source they were taken on;
+    bench.py reports whether that is the source of this build."""
+    b = _bench()
+    import json
+    d = json.load(open(b.PROFILE_JSON))
+    assert set(d["variants"]) >= {"spl4_minb3", "spl4_minb4"}
+    for v in d["variants"].values():
+        assert v["dram_bytes_per_eval"] > 0 and v["thread_inst_per_eval"] > 0
+    prof, current = b.kernel_profile("spl4_minb3")
+    assert prof["variant"] == "spl4_minb3"
+    assert current == (d["source_sha16"] == b.kernel_source_sha16())
