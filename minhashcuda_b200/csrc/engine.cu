@@ -565,14 +565,11 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
   // staging and sends 6.5-7 instead of 8 bytes per entry over the link.
   // Page-locked columns are copied by the DMA engine straight from the
   // caller: packing them would add host memory traffic the copy does not
-  // have (measured: 486 vs 448 ms per step on 2.8e9 entries), so they cross
+  // have (measured on 2.8e9 entries: 448 ms per step unpacked, 462 / 472 /
+  // 480 / 486 ms with 2, 4, 6 or 8 of every 8 blocks packed), so they cross
   // as they are.
-  // MHCUDA_B200_PIN_PACK_EIGHTHS = k packs k of every 8 blocks of page-locked
-  // input as well (measurement knob; 0 by default).
-  const int pin_pack_eighths = std::min(8, std::max(0, env_int("MHCUDA_B200_PIN_PACK_EIGHTHS", 0)));
   const int pack_bits =
-      (in.cols64 == 0 && (!pin_in || pin_pack_eighths > 0) &&
-       env_int("MHCUDA_B200_NO_PACK", 0) == 0)
+      (in.cols64 == 0 && !pin_in && env_int("MHCUDA_B200_NO_PACK", 0) == 0)
           ? (gen->dim <= (1u << 20) ? 4 : (gen->dim <= (1u << 24) ? 8 : 0))
           : 0;
   // Page-locked inputs copy straight from the caller: large blocks.  Pageable
@@ -695,9 +692,8 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
       MHB_CHECK(gen, sl.hc.ensure(static_cast<size_t>(n) * 4 + 512), mhcudaMemoryAllocationFailure);
     const size_t hi_off = packed_hi_offset(n);
     const size_t hi_bytes = pack_bits == 4 ? (static_cast<size_t>(n) + 1) / 2 : n;
-    const bool pack_this = pack_bits && n && (!pin_in || static_cast<int>(i % 8) < pin_pack_eighths);
     const bool packed =
-        pack_this &&
+        pack_bits && n &&
         stage_packed_cols(in, b0, n, sl.hc.as<uint16_t>(), sl.hc.as<uint8_t>() + hi_off, pack_bits);
     if (pin_in) {
       src_w = static_cast<const float *>(in.weights) + b0;
