@@ -179,7 +179,7 @@ struct MinhashCudaGenerator_ {
   struct Slot {
     DevBuf w, c, ip, out;
     PinnedBuf hw, hc, hip, hout;
-    cudaEvent_t h2d = nullptr, done = nullptr, d2h = nullptr, h2d2 = nullptr;
+    cudaEvent_t h2d = nullptr, done = nullptr, d2h = nullptr;
     bool busy = false;              // holds an enqueued block
     uint32_t *pending_out = nullptr;  // caller destination of a staged block of hashes
     size_t pending_bytes = 0;
@@ -189,7 +189,7 @@ struct MinhashCudaGenerator_ {
   // group's device work, so it keeps one more group in flight).
   static constexpr int kPipeSlots = 2, kBatchSlots = 3;
   mutable Slot slots[kBatchSlots];
-  mutable cudaStream_t s_in = nullptr, s_out = nullptr, s_in2 = nullptr;
+  mutable cudaStream_t s_in = nullptr, s_out = nullptr;
   // Autotuner results by shape class (see tune_key); read by every planner,
   // including the server's lane threads, hence its own lock.
   mutable std::mutex tune_mu;
@@ -220,12 +220,10 @@ struct MinhashCudaGenerator_ {
       if (sl.h2d) cudaEventDestroy(sl.h2d);
       if (sl.done) cudaEventDestroy(sl.done);
       if (sl.d2h) cudaEventDestroy(sl.d2h);
-      if (sl.h2d2) cudaEventDestroy(sl.h2d2);
       sl.w.release(); sl.c.release(); sl.ip.release(); sl.out.release();
       sl.hw.release(); sl.hc.release(); sl.hip.release(); sl.hout.release();
     }
     if (s_in) cudaStreamDestroy(s_in);
-    if (s_in2) cudaStreamDestroy(s_in2);
     if (s_out) cudaStreamDestroy(s_out);
     for (auto &g : graphs) cudaGraphExecDestroy(g.exec);
     d_chunk_owner.release(); d_batch_plan.release();
@@ -456,9 +454,7 @@ cudaError_t batch_streams(const Gen *gen) {
   if (gen->s_in) return cudaSuccess;
   cudaError_t e = cudaStreamCreateWithFlags(&gen->s_in, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&gen->s_out, cudaStreamNonBlocking);
-  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&gen->s_in2, cudaStreamNonBlocking);
   for (auto &sl : gen->slots) {
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.h2d2, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.h2d, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.d2h, cudaEventDisableTiming);
@@ -572,9 +568,6 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
   // have (measured on 2.8e9 entries: 448 ms per step unpacked, 462 / 472 /
   // 480 / 486 ms with 2, 4, 6 or 8 of every 8 blocks packed), so they cross
   // as they are.
-  // MHCUDA_B200_SPLIT_H2D=1: unpacked columns go over a second copy stream
-  // (measurement knob).
-  const bool split_in = env_int("MHCUDA_B200_SPLIT_H2D", 0) != 0;
   const int pack_bits =
       (in.cols64 == 0 && !pin_in && env_int("MHCUDA_B200_NO_PACK", 0) == 0)
           ? (gen->dim <= (1u << 20) ? 4 : (gen->dim <= (1u << 24) ? 8 : 0))
@@ -732,16 +725,12 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
                   mhcudaMemoryCopyError);
       } else {
         MHB_CHECK(gen, cudaMemcpyAsync(sl.c.ptr, src_c, static_cast<size_t>(n) * 4,
-                                       cudaMemcpyHostToDevice, split_in ? gen->s_in2 : gen->s_in),
+                                       cudaMemcpyHostToDevice, gen->s_in),
                   mhcudaMemoryCopyError);
       }
     }
     MHB_CHECK(gen, cudaEventRecord(sl.h2d, gen->s_in), mhcudaRuntimeError);
     MHB_CHECK(gen, cudaStreamWaitEvent(st, sl.h2d, 0), mhcudaRuntimeError);
-    if (split_in) {
-      MHB_CHECK(gen, cudaEventRecord(sl.h2d2, gen->s_in2), mhcudaRuntimeError);
-      MHB_CHECK(gen, cudaStreamWaitEvent(st, sl.h2d2, 0), mhcudaRuntimeError);
-    }
     const HashPlan plan = make_plan(gen, n, len, force);
     HashArgs a{};
     r = prepare_launch(gen, len, n, plan, &a);
