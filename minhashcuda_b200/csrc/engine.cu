@@ -179,11 +179,6 @@ struct MinhashCudaGenerator_ {
   struct Slot {
     DevBuf w, c, ip, out;
     PinnedBuf hw, hc, hip, hout;
-    // calc_pipelined: the slot's own launch scratch and compute stream, so
-    // that one block's kernels can start while the previous block's last
-    // wave is still running (slot 0 computes on the generator's stream).
-    DevBuf chunk_row, part_ln, part_kt;
-    cudaStream_t compute = nullptr;
     cudaEvent_t h2d = nullptr, done = nullptr, d2h = nullptr;
     bool busy = false;              // holds an enqueued block
     uint32_t *pending_out = nullptr;  // caller destination of a staged block of hashes
@@ -226,8 +221,6 @@ struct MinhashCudaGenerator_ {
       if (sl.done) cudaEventDestroy(sl.done);
       if (sl.d2h) cudaEventDestroy(sl.d2h);
       sl.w.release(); sl.c.release(); sl.ip.release(); sl.out.release();
-      sl.chunk_row.release(); sl.part_ln.release(); sl.part_kt.release();
-      if (sl.compute) cudaStreamDestroy(sl.compute);
       sl.hw.release(); sl.hc.release(); sl.hip.release(); sl.hout.release();
     }
     if (s_in) cudaStreamDestroy(s_in);
@@ -379,28 +372,6 @@ MHCUDAResult prepare_launch(const Gen *gen, uint32_t rows, uint32_t nnz, const H
   return mhcudaSuccess;
 }
 
-// prepare_launch with a pipeline slot's own scratch (the status word stays
-// the generator's: concurrent blocks only OR bits into it).
-MHCUDAResult prepare_slot_launch(const Gen *gen, Gen::Slot &sl, uint32_t rows, uint32_t nnz,
-                                 const HashPlan &plan, HashArgs *a) {
-  const MHCUDAResult r = prepare_launch(gen, rows, nnz, HashPlan{}, a);
-  if (r != mhcudaSuccess) return r;
-  const size_t slots = static_cast<size_t>(plan.nchunks) * 2;
-  MHB_CHECK(gen, sl.chunk_row.ensure(static_cast<size_t>(plan.nchunks) * 4),
-            mhcudaMemoryAllocationFailure);
-  MHB_CHECK(gen, sl.part_ln.ensure(slots * gen->s_pad * sizeof(float)),
-            mhcudaMemoryAllocationFailure);
-  MHB_CHECK(gen, sl.part_kt.ensure(slots * gen->s_pad * sizeof(uint2)),
-            mhcudaMemoryAllocationFailure);
-  a->chunk = plan.chunk;
-  a->nchunks = plan.nchunks;
-  a->ntiles = plan.ntiles;
-  a->chunk_row = sl.chunk_row.as<uint32_t>();
-  a->part_ln = sl.part_ln.as<float>();
-  a->part_kt = sl.part_kt.as<uint2>();
-  return mhcudaSuccess;
-}
-
 MHCUDAResult enqueue_hash(const Gen *gen, const HashArgs &a, const HashPlan &plan,
                           cudaStream_t stream, bool clear_status = true) {
   if (clear_status)
@@ -483,8 +454,6 @@ cudaError_t batch_streams(const Gen *gen) {
   if (gen->s_in) return cudaSuccess;
   cudaError_t e = cudaStreamCreateWithFlags(&gen->s_in, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&gen->s_out, cudaStreamNonBlocking);
-  for (int k = 1; k < Gen::kPipeSlots && e == cudaSuccess; ++k)
-    e = cudaStreamCreateWithFlags(&gen->slots[k].compute, cudaStreamNonBlocking);
   for (auto &sl : gen->slots) {
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.h2d, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming);
@@ -613,9 +582,7 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
   if (forced > 0) block_nnz = static_cast<uint64_t>(forced);
   const size_t row_bytes = static_cast<size_t>(gen->samples) * 2 * sizeof(uint32_t);
   MHB_CHECK(gen, gen->d_status.ensure(sizeof(uint32_t)), mhcudaMemoryAllocationFailure);
-  // Cleared on the copy stream: every block's kernels wait for their copies.
-  MHB_CHECK(gen, cudaMemsetAsync(gen->d_status.ptr, 0, sizeof(uint32_t), gen->s_in),
-            mhcudaRuntimeError);
+  MHB_CHECK(gen, cudaMemsetAsync(gen->d_status.ptr, 0, sizeof(uint32_t), st), mhcudaRuntimeError);
   // The blocks are cut from one matrix: a variant the autotuner chose for the
   // whole matrix's shape applies to each of them (their own, smaller shape
   // classes were never timed).
@@ -703,10 +670,8 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
     HashPlan big{};
     big.nchunks = max_chunks;
     HashArgs unused{};
-    for (int k = 0; k < Gen::kPipeSlots; ++k) {
-      const MHCUDAResult pr = prepare_slot_launch(gen, gen->slots[k], 0, 0, big, &unused);
-      if (pr != mhcudaSuccess) return pr;
-    }
+    const MHCUDAResult pr = prepare_launch(gen, 0, 0, big, &unused);
+    if (pr != mhcudaSuccess) return pr;
   }
 
   MHCUDAResult r = mhcudaSuccess;
@@ -764,15 +729,11 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
                   mhcudaMemoryCopyError);
       }
     }
-    // Each slot computes on its own stream with its own scratch: this block's
-    // kernels start while the previous block's last wave is still running.
-    const cudaStream_t cst =
-        sl.compute && env_int("MHCUDA_B200_PIPE_ONE_STREAM", 0) == 0 ? sl.compute : st;
     MHB_CHECK(gen, cudaEventRecord(sl.h2d, gen->s_in), mhcudaRuntimeError);
-    MHB_CHECK(gen, cudaStreamWaitEvent(cst, sl.h2d, 0), mhcudaRuntimeError);
+    MHB_CHECK(gen, cudaStreamWaitEvent(st, sl.h2d, 0), mhcudaRuntimeError);
     const HashPlan plan = make_plan(gen, n, len, force);
     HashArgs a{};
-    r = prepare_slot_launch(gen, sl, len, n, plan, &a);
+    r = prepare_launch(gen, len, n, plan, &a);
     if (r != mhcudaSuccess) break;
     a.weights = sl.w.as<float>();
     if (packed) {
@@ -784,9 +745,9 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
     }
     a.indptr = sl.ip.as<uint32_t>();
     a.out = sl.out.as<uint32_t>();
-    r = enqueue_hash(gen, a, plan, cst, /*clear_status=*/false);
+    r = enqueue_hash(gen, a, plan, st, /*clear_status=*/false);
     if (r != mhcudaSuccess) break;
-    MHB_CHECK(gen, cudaEventRecord(sl.done, cst), mhcudaRuntimeError);
+    MHB_CHECK(gen, cudaEventRecord(sl.done, st), mhcudaRuntimeError);
     MHB_CHECK(gen, cudaStreamWaitEvent(gen->s_out, sl.done, 0), mhcudaRuntimeError);
     uint32_t *dst = output + static_cast<size_t>(r0) * gen->samples * 2;
     if (pin_out) {
