@@ -61,6 +61,12 @@ def test_host_side_validation_without_gpu():
                            one.ctypes.data) == mb.INVALID_ARGUMENTS
     assert lib.mhcuda_retrieve_random_vars(None, None, None, None) == mb.INVALID_ARGUMENTS
     assert lib.mhcuda_assign_random_vars(None, None, None, None) == mb.INVALID_ARGUMENTS
+    # Added entry points refuse null arguments before touching a device.
+    assert lib.mhcuda_calc_batch_device(None, 1, None, None, None, None, None,
+                                        None) == mb.INVALID_ARGUMENTS
+    assert lib.mhcuda_host_register(0, None, 16) == mb.INVALID_ARGUMENTS
+    assert lib.mhcuda_host_register(0, one.ctypes.data, 0) == mb.INVALID_ARGUMENTS
+    assert lib.mhcuda_host_unregister(0, None) == mb.INVALID_ARGUMENTS
     assert lib.mhcuda_calc_batch(None, 0, None, None, None, None, None) == mb.INVALID_ARGUMENTS
     assert lib.mhcuda_calc_typed(None, one.ctypes.data, mb.FLOAT64, one.ctypes.data, mb.INT64,
                                  one.ctypes.data, mb.INT64, 1, one.ctypes.data) == \
