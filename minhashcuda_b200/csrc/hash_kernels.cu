@@ -1002,14 +1002,7 @@ HashFn pick_hash(uint32_t spl, uint32_t minb, uint32_t s_pad, bool packed = fals
 cudaError_t launch_hash(const HashArgs &a, const HashPlan &plan, cudaStream_t stream) {
   const HashFn fn = pick_hash(plan.spl, plan.minb, a.s_pad, a.col_hi_bits != 0);
   if (!fn) return cudaErrorInvalidValue;
-  if (plan.dyn_smem) {
-    // Unused dynamic shared memory: reserves room on each SM, so fewer blocks
-    // of this launch are resident at once.
-    const cudaError_t e = cudaFuncSetAttribute(
-        fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(plan.dyn_smem));
-    if (e != cudaSuccess) return e;
-  }
-  fn<<<plan.grid, kHashBlock, plan.dyn_smem, stream>>>(a);
+  fn<<<plan.grid, kHashBlock, 0, stream>>>(a);
   return cudaGetLastError();
 }
 

@@ -128,9 +128,6 @@ struct MinhashCudaServer_ {
   // batches retire their blocks sooner, so a small batch's blocks find SMs
   // sooner.
   uint32_t min_items_high = 2, min_items_low = 2;
-  // Unused dynamic shared memory per block of a large batch's hash launch
-  // (MHCUDA_B200_SERVER_LOW_SMEM bytes; 0: none).
-  uint32_t low_dyn_smem = 0;
   uint32_t max_low_inflight = 6;            // low-priority batches out at once (lanes - 2)
   uint64_t zero_copy_max_bytes = ~0ull;     // CSR bytes of a batch read from mapped memory
   uint32_t low_inflight = 0;
@@ -328,9 +325,6 @@ MHCUDAResult MinhashCudaServer_::run_units(Lane &lane, const std::vector<Unit> &
     const uint64_t resident = static_cast<uint64_t>(sm_count) * bps;
     plan.grid = static_cast<uint32_t>(std::max<uint64_t>(
         1, high ? std::min(blocks, resident) : std::min<uint64_t>(blocks, 1u << 30)));
-    // Large batches may reserve shared memory they do not use, so that fewer
-    // of their blocks fit an SM and small batches' blocks find room at once.
-    if (!high) plan.dyn_smem = low_dyn_smem;
   }
   mhb::HashArgs a{};
   a.params = g.params;
@@ -602,8 +596,6 @@ MinhashCudaServer *mhcuda_server_start(uint32_t devices, uint64_t hbm_budget_byt
       static_cast<uint32_t>(env_u64("MHCUDA_B200_SERVER_MIN_ITEMS_HIGH", srv->min_items_high));
   srv->min_items_low =
       static_cast<uint32_t>(env_u64("MHCUDA_B200_SERVER_MIN_ITEMS_LOW", srv->min_items_low));
-  srv->low_dyn_smem = static_cast<uint32_t>(
-      std::min<uint64_t>(env_u64("MHCUDA_B200_SERVER_LOW_SMEM", 0), 160u << 10));
   srv->max_low_inflight = static_cast<uint32_t>(std::min<uint64_t>(
       lanes, env_u64("MHCUDA_B200_SERVER_LOW_INFLIGHT", lanes > 2 ? lanes - 2 : 1)));
   cudaDeviceGetAttribute(&srv->sm_count, cudaDevAttrMultiProcessorCount, dev);

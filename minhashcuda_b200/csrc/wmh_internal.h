@@ -44,7 +44,6 @@ struct HashPlan {
   uint32_t minb;     // kernel variant: minimum resident blocks per SM (4, or 3 for spl 4)
   uint32_t ntiles;   // sample tiles of 32*spl samples
   uint32_t grid;     // persistent grid (blocks of kHashBlock threads)
-  uint32_t dyn_smem; // extra dynamic shared memory per block (caps blocks per SM; 0: none)
 };
 
 constexpr int kHashBlock = 256;
