@@ -568,9 +568,6 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
   // have (measured on 2.8e9 entries: 448 ms per step unpacked, 462 / 472 /
   // 480 / 486 ms with 2, 4, 6 or 8 of every 8 blocks packed), so they cross
   // as they are.
-  // Row blocks in flight (MHCUDA_B200_PIPE_SLOTS, 2 or 3).
-  const int pipe_slots =
-      std::min(Gen::kBatchSlots, std::max(2, env_int("MHCUDA_B200_PIPE_SLOTS", Gen::kPipeSlots)));
   const int pack_bits =
       (in.cols64 == 0 && !pin_in && env_int("MHCUDA_B200_NO_PACK", 0) == 0)
           ? (gen->dim <= (1u << 20) ? 4 : (gen->dim <= (1u << 24) ? 8 : 0))
@@ -656,7 +653,7 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
       max_len = std::max<uint64_t>(max_len, b.r1 - b.r0);
       max_chunks = std::max(max_chunks, make_plan(gen, n, b.r1 - b.r0, force).nchunks);
     }
-    for (int k = 0; k < pipe_slots; ++k) {
+    for (int k = 0; k < Gen::kPipeSlots; ++k) {
       Gen::Slot &sl = gen->slots[k];
       MHB_CHECK(gen, sl.w.ensure(max_n * 4 + 16), mhcudaMemoryAllocationFailure);
       MHB_CHECK(gen, sl.c.ensure(max_n * 4 + 512), mhcudaMemoryAllocationFailure);
@@ -680,7 +677,7 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
   MHCUDAResult r = mhcudaSuccess;
   for (uint32_t i = 0; i < blocks.size() && r == mhcudaSuccess; ++i) {
     const uint32_t r0 = blocks[i].r0, r1 = blocks[i].r1;
-    Gen::Slot &sl = gen->slots[i % pipe_slots];
+    Gen::Slot &sl = gen->slots[i % Gen::kPipeSlots];
     r = retire(sl);
     if (r != mhcudaSuccess) break;
     const uint32_t len = r1 - r0;
