@@ -658,7 +658,7 @@ def run_ingest(args, rank, world, local):
         print(json.dumps(line), flush=True)
 
 
-def run_streamed(args, rank, world, local, emit=True, passes=None):
+def run_streamed(args, rank, world, local, emit=True, n_passes=None):
     """Row-streamed wide generator: 12,000,000 dims x 128 samples (18.4 GB of
     parameters resident), 10,000,000 rows hashed as 19 blocks of 524,288 rows
     plus one of 38,528, each block an mhcuda_calc call on page-locked host
@@ -713,7 +713,7 @@ def run_streamed(args, rank, world, local, emit=True, passes=None):
     # is ~1.4 s of host<->device traffic, exposed to other users of the host).
     passes = []
     with Clocks(local) as clk:
-        for _ in range(max(1, passes or args.steps)):
+        for _ in range(max(1, n_passes or args.steps)):
             t = time.perf_counter()
             evals = sum(run_block(k, rows) for k, rows in schedule)
             passes.append(time.perf_counter() - t)
@@ -1007,7 +1007,7 @@ def run_extras(args, rank, world, local, lib, peak, peak_kind):
              "batched_over_plain", "bit_exact_plain_vs_batched",
              "bit_exact_plain_vs_device_batch", "rows_per_s", "e2e"]),
         "streamed": lambda: summary(
-            run_streamed(args, rank, world, local, emit=False, passes=2),
+            run_streamed(args, rank, world, local, emit=False, n_passes=3),
             ["value", "unit", "config", "rows_per_s", "seconds_total", "pass_seconds",
              "device_resident", "streamed_equals_device_path", "e2e"]),
         "serving": lambda: summary(
