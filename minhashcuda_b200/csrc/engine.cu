@@ -309,7 +309,7 @@ HashPlan make_plan(const Gen *gen, uint64_t nnz, uint64_t rows, const TuneChoice
   p.minb = 4;
   if (p.spl == 4) {
     const int minb = env_int("MHCUDA_B200_MINB", have_tuned ? static_cast<int>(tuned.minb) : 4);
-    p.minb = minb == 3 ? 3u : 4u;
+    p.minb = (minb == 3 || minb == 2) ? static_cast<uint32_t>(minb) : 4u;
   }
   const uint32_t tile_w = 32u * p.spl;
   p.ntiles = (s_pad + tile_w - 1) / tile_w;
@@ -1407,12 +1407,14 @@ enum MHCUDAResult mhcuda_autotune(const MinhashCudaGenerator *gen, const float *
   MHB_ON_DEVICE(gen);
   const cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : gen->stream;
   // Candidates: samples per lane (lane utilisation of the last tile >= 1/2),
-  // register budget of the 4-sample variant, and chunk granularity.
+  // register budget of the 4-sample variant (4, 3 or 2 resident blocks per SM:
+  // fewer warps with more registers win where the gathers hit L2, more warps
+  // where they stream from HBM), and chunk granularity.
   std::vector<TuneChoice> cands;
   for (uint32_t spl : {4u, 2u, 1u}) {
     const uint32_t w = 32u * spl, tiles = (gen->s_pad + w - 1) / w;
     if (static_cast<double>(gen->s_pad) / (static_cast<double>(tiles) * w) < 0.5) continue;
-    for (uint32_t minb : spl == 4 ? std::vector<uint32_t>{4u, 3u} : std::vector<uint32_t>{4u})
+    for (uint32_t minb : spl == 4 ? std::vector<uint32_t>{4u, 3u, 2u} : std::vector<uint32_t>{4u})
       for (uint32_t waves : {8u, 32u, 128u}) cands.push_back(TuneChoice{spl, minb, waves});
   }
   cudaEvent_t e0 = nullptr, e1 = nullptr;

@@ -946,14 +946,17 @@ BatchFn pick_batch(uint32_t spl, uint32_t minb, uint32_t s_pad) {
   switch (spl * 100000 + minb * 10000 + s_pad) {
     case 440128: return hash_batch_kernel<4, 4, 128>;
     case 430128: return hash_batch_kernel<4, 3, 128>;
+    case 420128: return hash_batch_kernel<4, 2, 128>;
     case 440256: return hash_batch_kernel<4, 4, 256>;
     case 430256: return hash_batch_kernel<4, 3, 256>;
+    case 420256: return hash_batch_kernel<4, 2, 256>;
     case 240064: return hash_batch_kernel<2, 4, 64>;
     default: break;
   }
   switch (spl * 10 + minb) {
     case 44: return hash_batch_kernel<4, 4, 0>;
     case 43: return hash_batch_kernel<4, 3, 0>;
+    case 42: return hash_batch_kernel<4, 2, 0>;
     case 24: return hash_batch_kernel<2, 4, 0>;
     case 14: return hash_batch_kernel<1, 4, 0>;
     default: return nullptr;
@@ -967,14 +970,17 @@ HashFn pick_hash(uint32_t spl, uint32_t minb, uint32_t s_pad, bool packed = fals
     switch (spl * 100000 + minb * 10000 + s_pad) {
       case 440128: return hash_kernel<4, 4, 128, true>;
       case 430128: return hash_kernel<4, 3, 128, true>;
+      case 420128: return hash_kernel<4, 2, 128, true>;
       case 440256: return hash_kernel<4, 4, 256, true>;
       case 430256: return hash_kernel<4, 3, 256, true>;
+      case 420256: return hash_kernel<4, 2, 256, true>;
       case 240064: return hash_kernel<2, 4, 64, true>;
       default: break;
     }
     switch (spl * 10 + minb) {
       case 44: return hash_kernel<4, 4, 0, true>;
       case 43: return hash_kernel<4, 3, 0, true>;
+      case 42: return hash_kernel<4, 2, 0, true>;
       case 24: return hash_kernel<2, 4, 0, true>;
       case 14: return hash_kernel<1, 4, 0, true>;
       default: return nullptr;
@@ -983,14 +989,17 @@ HashFn pick_hash(uint32_t spl, uint32_t minb, uint32_t s_pad, bool packed = fals
   switch (spl * 100000 + minb * 10000 + s_pad) {
     case 440128: return hash_kernel<4, 4, 128, false>;
     case 430128: return hash_kernel<4, 3, 128, false>;
+    case 420128: return hash_kernel<4, 2, 128, false>;
     case 440256: return hash_kernel<4, 4, 256, false>;
     case 430256: return hash_kernel<4, 3, 256, false>;
+    case 420256: return hash_kernel<4, 2, 256, false>;
     case 240064: return hash_kernel<2, 4, 64, false>;
     default: break;
   }
   switch (spl * 10 + minb) {
     case 44: return hash_kernel<4, 4, 0, false>;
     case 43: return hash_kernel<4, 3, 0, false>;
+    case 42: return hash_kernel<4, 2, 0, false>;
     case 24: return hash_kernel<2, 4, 0, false>;
     case 14: return hash_kernel<1, 4, 0, false>;
     default: return nullptr;

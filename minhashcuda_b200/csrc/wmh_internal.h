@@ -41,7 +41,7 @@ struct HashPlan {
   uint32_t chunk;    // positions per chunk, multiple of 32
   uint32_t nchunks;  // >= 1
   uint32_t spl;      // samples per lane in one item: 1, 2 or 4
-  uint32_t minb;     // kernel variant: minimum resident blocks per SM (4, or 3 for spl 4)
+  uint32_t minb;     // kernel variant: minimum resident blocks per SM (4; 3 or 2 for spl 4)
   uint32_t ntiles;   // sample tiles of 32*spl samples
   uint32_t grid;     // persistent grid (blocks of kHashBlock threads)
 };
