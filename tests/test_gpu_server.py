@@ -195,3 +195,29 @@ def test_page_locked_requests_copy_directly():
         del keep
     finally:
         _fini(gens)
+
+
+def test_stage_trace_has_one_row_per_request(monkeypatch, tmp_path):
+    """MHCUDA_B200_SERVER_TRACE: when the server stops, every completed request
+    has a CSV row whose stage times add up to its total latency."""
+    import csv
+    from minhashcuda_b200.server import Server
+    rng = np.random.default_rng(8)
+    gens = _gens([(2000, 128)], rng)
+    trace = tmp_path / "trace.csv"
+    monkeypatch.setenv("MHCUDA_B200_SERVER_TRACE", str(trace))
+    try:
+        g = gens[0]
+        reqs = [random_csr(rng, int(rng.integers(1, 400)), g[1], 40) for _ in range(25)]
+        with Server(hbm_budget=256 << 20, lanes=2) as srv:
+            for t in [srv.submit(g[0], m) for m in reqs]:
+                srv.wait(t)
+        rows = list(csv.DictReader(open(trace)))
+        assert len(rows) == len(reqs)
+        assert sorted(int(r["rows"]) for r in rows) == sorted(m.shape[0] for m in reqs)
+        for r in rows:
+            parts = sum(float(r[k]) for k in ("queued_ms", "gather_launch_ms", "device_ms",
+                                              "complete_ms"))
+            assert abs(parts - float(r["total_ms"])) < 0.01 and float(r["total_ms"]) > 0
+    finally:
+        _fini(gens)
