@@ -132,6 +132,17 @@ struct TuneChoice {
   uint32_t waves = 32;
 };
 
+// The autotuner's two choices for a shape class.  `alone` is the fastest
+// candidate of all; `streamed` the fastest with 3 or 4 resident blocks per SM,
+// for launches that run beside host<->device copies (the mhcuda_calc
+// pipeline): the copies share HBM with the kernel's gathers and lengthen their
+// latency, which the 2-block budget, with half the resident warps, hides worst
+// (on a 2,000,000-row Zipf matrix its blocks were 7% slower end to end than
+// 4-block ones, although 3% faster alone).
+struct TunedShape {
+  TuneChoice alone, streamed;
+};
+
 // A captured plan/hash/finalize sequence, replayed for identical calls.
 struct GraphEntry {
   std::vector<unsigned char> key;
@@ -193,7 +204,7 @@ struct MinhashCudaGenerator_ {
   // Autotuner results by shape class (see tune_key); read by every planner,
   // including the server's lane threads, hence its own lock.
   mutable std::mutex tune_mu;
-  mutable std::unordered_map<uint64_t, TuneChoice> tuned;
+  mutable std::unordered_map<uint64_t, TunedShape> tuned;
   // CUDA graphs of mhcuda_calc_device calls, most recent last.
   mutable std::vector<GraphEntry> graphs;
   // Device-resident batches, most recent last, and their batch-wide scratch.
@@ -266,12 +277,14 @@ uint64_t tune_key(uint64_t nnz, uint64_t rows) {
   return (lg(nnz + 1) << 8) | lg(avg + 1);
 }
 
-// The autotuner's choice for launches of this shape class, if it has one.
-bool tuned_choice(const Gen *gen, uint64_t nnz, uint64_t rows, TuneChoice *out) {
+// The autotuner's choice for launches of this shape class, if it has one
+// (streamed: the one for launches beside host<->device copies).
+bool tuned_choice(const Gen *gen, uint64_t nnz, uint64_t rows, TuneChoice *out,
+                  bool streamed = false) {
   std::lock_guard<std::mutex> lock(gen->tune_mu);
   const auto it = gen->tuned.find(tune_key(nnz, rows));
   if (it == gen->tuned.end()) return false;
-  *out = it->second;
+  *out = streamed ? it->second.streamed : it->second.alone;
   return true;
 }
 
@@ -585,9 +598,9 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
   MHB_CHECK(gen, cudaMemsetAsync(gen->d_status.ptr, 0, sizeof(uint32_t), st), mhcudaRuntimeError);
   // The blocks are cut from one matrix: a variant the autotuner chose for the
   // whole matrix's shape applies to each of them (their own, smaller shape
-  // classes were never timed).
+  // classes were never timed), its choice for launches beside copies.
   TuneChoice whole{};
-  const TuneChoice *force = tuned_choice(gen, nnz, length, &whole) ? &whole : nullptr;
+  const TuneChoice *force = tuned_choice(gen, nnz, length, &whole, true) ? &whole : nullptr;
 
   // Finishes a slot: waits for its hashes and moves staged ones to the caller.
   auto retire = [&](Gen::Slot &sl) -> MHCUDAResult {
@@ -1420,8 +1433,8 @@ enum MHCUDAResult mhcuda_autotune(const MinhashCudaGenerator *gen, const float *
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   MHB_CHECK(gen, cudaEventCreate(&e0), mhcudaRuntimeError);
   MHB_CHECK(gen, cudaEventCreate(&e1), mhcudaRuntimeError);
-  TuneChoice best{};
-  double best_t = 1e300;
+  TuneChoice best{}, best_streamed{};
+  double best_t = 1e300, best_streamed_t = 1e300;
   MHCUDAResult r = mhcudaSuccess;
   for (const TuneChoice &c : cands) {
     const HashPlan plan = make_plan(gen, nnz, length, &c);
@@ -1445,13 +1458,17 @@ enum MHCUDAResult mhcuda_autotune(const MinhashCudaGenerator *gen, const float *
       best_t = ms / 2;
       best = c;
     }
+    if (c.minb != 2 && ms / 2 < best_streamed_t) {
+      best_streamed_t = ms / 2;
+      best_streamed = c;
+    }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (r != mhcudaSuccess) return r;
   {
     std::lock_guard<std::mutex> tl(gen->tune_mu);
-    gen->tuned[tune_key(nnz, length)] = best;
+    gen->tuned[tune_key(nnz, length)] = TunedShape{best, best_streamed};
   }
   if (choice) {
     choice[0] = best.spl;

@@ -33,6 +33,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cstdint>
+#include <cstdlib>
 
 #include "wmh_internal.h"
 
@@ -194,8 +195,8 @@ constexpr uint32_t kSpinLimit = 1u << 22;
 
 // One warp's staging area: two windows of weights (turned into ln w in
 // place) and column indices, each with its own transaction barrier.  Column
-// slot n of a window of n positions holds column 0, so the loop may prefetch
-// one position past the window without a bounds branch (the row stride of c,
+// slots n and n + 1 of a window of n positions hold column 0, so the loop may
+// prefetch two positions past the window without a bounds branch (the row stride of c,
 // kWin + 4 words, keeps both windows 16-byte aligned for the bulk copies).
 struct alignas(16) WarpStage {
   float w[2][kWin];
@@ -341,7 +342,7 @@ __device__ __forceinline__ bool finish_window(const HashArgs &a, WarpStage &st, 
     st.w[b][i] = logf(x);
   }
   if (__any_sync(0xFFFFFFFFu, bad) && lane == 0) atomicOr(a.status, kStatusBadColumn);
-  if (lane == 0) st.c[b][n] = 0;  // the prefetch slot past the window
+  if (lane == 0) st.c[b][n] = st.c[b][n + 1] = 0;  // the prefetch slots past the window
   __syncwarp();
   return true;
 }
@@ -487,6 +488,17 @@ __device__ __forceinline__ void warp_ctx_init(WarpCtx &w, WarpStage *stage_all,
   w.parity = 0;
 }
 
+// Parameter sets a warp keeps in registers for register budget MINB
+// (resident blocks per SM).  The gathers are latency-bound; with 2 blocks per
+// SM there are half the warps of the 4-block budget to hide them, and 128
+// registers per thread, room for a third set (12 registers at 4 samples per
+// lane) that keeps two positions' gathers in flight: 114-118 registers, no
+// spills.  At 524,288 rows of the 1,000,000-dim Zipf(1.1) matrix this took
+// the 2-block kernel from 107.6 to 101.9 ms (4 blocks: 105.6 ms); on uniform
+// columns over 12,000,000 dims from 75.1 to 65.0 ms (4 blocks: 61.6 ms).  The
+// 3- and 4-block budgets (85 and 64 registers) have no room for it.
+__host__ __device__ constexpr int param_depth(int minb) { return minb == 2 ? 3 : 2; }
+
 // One (chunk c, sample tile) item over the CSR of `a`: finishes the rows
 // that lie inside chunk c and leaves partial minima for the rows that cross
 // its ends.  Returns false after an error exit (status flagged, in-flight
@@ -494,7 +506,9 @@ __device__ __forceinline__ void warp_ctx_init(WarpCtx &w, WarpStage *stage_all,
 // SPAD: the generator's s_pad when it is known at compile time (0: read it
 // from the arguments), which turns the parameter-block addressing into one
 // wide multiply-add and immediate load offsets.
-template <int SPL, int SPAD, bool PACKED>
+// DEPTH: parameter sets in registers, 2 (the next position is loaded while
+// one is evaluated) or 3 (the next two are), see param_depth.
+template <int SPL, int SPAD, bool PACKED, int DEPTH>
 __device__ __forceinline__ bool hash_item(const HashArgs &a, uint32_t c, uint32_t tile,
                                           WarpCtx &wc) {
   const uint32_t lane = wc.lane;
@@ -576,8 +590,59 @@ __device__ __forceinline__ bool hash_item(const HashArgs &a, uint32_t c, uint32_
       const float *__restrict__ lw = stg.w[b];
       const uint32_t *__restrict__ cl = stg.c[b];
 
-      // Columns in the window are < dim, and slot n holds column 0
+      // Columns in the window are < dim, and slots n and n + 1 hold column 0
       // (finish_window).
+      if constexpr (DEPTH == 3) {
+        // Three parameter sets: at each segment's start A holds position i
+        // and B position i + 1; positions up to n + 1 read the zero column
+        // slots past the window.
+        Params<SPL> A, B, C;
+        A.load(pbase + cl[0] * col_stride, spad);
+        B.load(pbase + cl[1] * col_stride, spad);
+        uint32_t i = 0;
+        while (i < n) {
+          while (ws + i >= row_end) {
+            flush();
+            if (r_next >= r_stop) {  // only reachable with inconsistent offsets
+              if (lane == 0) atomicOr(a.status, kStatusBadIndptr);
+              drain(k + 1);
+              return false;
+            }
+            row = r_next++;
+            row_end = a.indptr[row + 1] - base;
+            head = false;
+            st.reset();
+          }
+          const uint32_t seg = min(row_end - ws, n);
+          while (i + 3 <= seg) {  // prefetches reach i + 4 <= n + 1
+            C.load(pbase + cl[i + 2] * col_stride, spad);
+            eval_all<SPL>(A, lw[i], ws + i, active, st);
+            A.load(pbase + cl[i + 3] * col_stride, spad);
+            eval_all<SPL>(B, lw[i + 1], ws + i + 1, active, st);
+            B.load(pbase + cl[i + 4] * col_stride, spad);
+            eval_all<SPL>(C, lw[i + 2], ws + i + 2, active, st);
+            i += 3;
+          }
+          if (i + 2 == seg) {
+            C.load(pbase + cl[i + 2] * col_stride, spad);
+            eval_all<SPL>(A, lw[i], ws + i, active, st);
+            eval_all<SPL>(B, lw[i + 1], ws + i + 1, active, st);
+            i += 2;
+            A = C;
+            B.load(pbase + cl[i + 1] * col_stride, spad);
+          } else if (i + 1 == seg) {
+            eval_all<SPL>(A, lw[i], ws + i, active, st);
+            i += 1;
+            A = B;
+            B.load(pbase + cl[i + 1] * col_stride, spad);
+          }
+        }
+        if (k + 2 < nwin) {
+          const uint32_t ws2 = ws + 2 * kWin;
+          issue_window<PACKED>(a, stg, pk, b, ws2, min(kWin, ce - ws2), bulk_ok, lane);
+        }
+        continue;
+      }
       Params<SPL> A, B;
       uint32_t dA = cl[0], dB = 0;
       A.load(pbase + dA * col_stride, spad);
@@ -653,7 +718,7 @@ __global__ void __launch_bounds__(kHashBlock, MINB) hash_kernel(const HashArgs a
   const uint32_t items = a.nchunks * a.ntiles;
   for (uint32_t item = gw; item < items; item += nw) {
     const uint32_t c = item / a.ntiles;
-    if (!hash_item<SPL, SPAD, PACKED>(a, c, item - c * a.ntiles, wc)) return;
+    if (!hash_item<SPL, SPAD, PACKED, param_depth(MINB)>(a, c, item - c * a.ntiles, wc)) return;
   }
 }
 
@@ -900,7 +965,8 @@ __global__ void __launch_bounds__(kHashBlock, MINB) hash_batch_kernel(const Batc
     __syncwarp();
     if (wc.lane == 0) view = matrix_view(b, b.mats[m], chunk);
     __syncwarp();
-    if (!hash_item<SPL, SPAD, false>(view, gc - base, item - gc * ntiles, wc)) return;
+    if (!hash_item<SPL, SPAD, false, param_depth(MINB)>(view, gc - base, item - gc * ntiles, wc))
+      return;
   }
 }
 

@@ -82,6 +82,15 @@ def test_autotune_choice_is_used_and_exact():
                                       m.shape[0], m.nnz, out.data_ptr(), None) == 0
         assert lib.mhcuda_device_status(g) == 0
         np.testing.assert_array_equal(out.cpu().numpy().view(np.uint32), want)
+        # Host buffers: the copy pipeline applies the choice made for
+        # launches beside copies.
+        hw = np.ascontiguousarray(m.data, np.float32)
+        hc = np.ascontiguousarray(m.indices, np.uint32)
+        hr = np.ascontiguousarray(m.indptr, np.uint32)
+        hout = np.zeros((m.shape[0], samples, 2), np.uint32)
+        assert lib.mhcuda_calc(g, hw.ctypes.data, hc.ctypes.data, hr.ctypes.data, m.shape[0],
+                               hout.ctypes.data) == 0
+        np.testing.assert_array_equal(hout, want)
     finally:
         lib.mhcuda_fini(g)
 
