@@ -67,7 +67,7 @@ enum MHCUDAResult mhcuda_device_status(const MinhashCudaGenerator *gen);
  *    mhcudaInvalidArguments when ceil(nnz / 2^20) chunks do not fit in
  *    8 MiB - 1 KiB (about 2.8e9 nnz at 128 samples, 5*2^20 at 65535).
  *  - The first call on a device looks up the array's device address and
- *    caches it; make that first call before any stream capture begins.
+ *    caches it.
  *  - All calls share the array, which keeps the last call's contents: the
  *    status word is cleared by every call and everything else a call reads it
  *    writes first.  Calls whose work overlapped on the GPU would race on the

@@ -27,8 +27,7 @@
 //    for its own work to finish before returning and calls are serialised by a
 //    process-wide lock;
 //  - the first call on a device looks up the array's device address (with
-//    that device current) and caches it; make that first call before any
-//    stream capture begins.
+//    that device current) and caches it.
 #include <algorithm>
 #include <cstdio>
 #include <mutex>
