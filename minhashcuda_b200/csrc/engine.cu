@@ -20,6 +20,7 @@
 #include <cstring>
 #include <memory>
 #include <mutex>
+#include <string>
 #include <thread>
 #include <unordered_map>
 #include <vector>
@@ -195,10 +196,11 @@ struct MinhashCudaGenerator_ {
     uint32_t *pending_out = nullptr;  // caller destination of a staged block of hashes
     size_t pending_bytes = 0;
   };
-  // Pipelines: calc_pipelined uses the first kPipeSlots, mhcuda_calc_batch
-  // all kBatchSlots (its host gather/scatter per group is as long as the
-  // group's device work, so it keeps one more group in flight).
-  static constexpr int kPipeSlots = 2, kBatchSlots = 3;
+  // Pipelines: calc_pipelined and mhcuda_calc_batch use all three slots, so a
+  // block's copy-in never waits for the copy-out of the block two before it
+  // (and a batch group's host gather/scatter, as long as its device work,
+  // overlaps the groups on either side).
+  static constexpr int kPipeSlots = 3, kBatchSlots = 3;
   mutable Slot slots[kBatchSlots];
   mutable cudaStream_t s_in = nullptr, s_out = nullptr;
   // Autotuner results by shape class (see tune_key); read by every planner,
@@ -561,6 +563,66 @@ bool stage_packed_cols(const HostCsr &in, uint64_t b0, size_t n, uint16_t *lo, u
 // buffer (16-byte aligned for the kernel's bulk copies).
 size_t packed_hi_offset(size_t n) { return (2 * n + 255) & ~static_cast<size_t>(255); }
 
+// Per-block timeline of calc_pipelined, written when MHCUDA_B200_PIPE_TRACE
+// names a file: one CSV line per row block with its nnz and, in ms from the
+// start of the call's first copy-in, the start and end of its copy-in,
+// hashing (plan + hash + finalize) and copy-out, from CUDA events on the
+// copy-in, generator and copy-out streams.  Lines are appended; `call`
+// counts the traced calls of the process.
+class PipeTrace {
+ public:
+  enum Point { kH2dStart, kH2dEnd, kHashStart, kHashEnd, kD2hStart, kD2hEnd, kPoints };
+  explicit PipeTrace(size_t blocks) {
+    const char *p = getenv("MHCUDA_B200_PIPE_TRACE");
+    if (!p || !*p) return;
+    path_ = p;
+    ev_.assign(blocks * kPoints, nullptr);
+    nnz_.assign(blocks, 0);
+    for (auto &e : ev_)
+      if (cudaEventCreate(&e) != cudaSuccess) {
+        e = nullptr;
+        path_.clear();  // no trace rather than a partial one
+      }
+  }
+  ~PipeTrace() {
+    for (auto &e : ev_)
+      if (e) cudaEventDestroy(e);
+  }
+  bool on() const { return !path_.empty(); }
+  void mark(size_t block, Point pt, cudaStream_t s) {
+    if (on()) cudaEventRecord(ev_[block * kPoints + pt], s);
+  }
+  void nnz(size_t block, uint64_t n) {
+    if (on()) nnz_[block] = n;
+  }
+  // After every block has been retired (their events have completed).
+  void write(size_t issued) {
+    if (!on() || issued == 0) return;
+    static std::atomic<int> calls{0};
+    const int call = calls++;
+    FILE *f = fopen(path_.c_str(), "a");
+    if (!f) return;
+    if (ftell(f) == 0) fprintf(f, "call,block,nnz,h2d_start,h2d_end,hash_start,hash_end,d2h_start,d2h_end\n");
+    for (size_t b = 0; b < issued; ++b) {
+      fprintf(f, "%d,%zu,%" PRIu64, call, b, nnz_[b]);
+      for (int pt = 0; pt < kPoints; ++pt) {
+        float ms = -1.0f;
+        if (cudaEventSynchronize(ev_[b * kPoints + pt]) != cudaSuccess ||
+            cudaEventElapsedTime(&ms, ev_[0], ev_[b * kPoints + pt]) != cudaSuccess)
+          ms = -1.0f;
+        fprintf(f, ",%.3f", ms);
+      }
+      fprintf(f, "\n");
+    }
+    fclose(f);
+  }
+
+ private:
+  std::string path_;
+  std::vector<cudaEvent_t> ev_;
+  std::vector<uint64_t> nnz_;
+};
+
 MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
                             uint32_t *output) {
   const cudaStream_t st = gen->stream;
@@ -585,11 +647,17 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
       (in.cols64 == 0 && !pin_in && env_int("MHCUDA_B200_NO_PACK", 0) == 0)
           ? (gen->dim <= (1u << 20) ? 4 : (gen->dim <= (1u << 24) ? 8 : 0))
           : 0;
-  // Page-locked inputs copy straight from the caller: large blocks.  Pageable
-  // ones go through pinned staging, which is cheaper to allocate (and
-  // re-fill) in smaller blocks.
+  // Block size once the pipeline has ramped up.  A block's copy-in (8 B per
+  // nnz over a Gen5 x16 link) and its hashing (128 samples) take about as
+  // long, so the kernel waits for every block that is larger than the one
+  // before it; a smaller steady block shortens the ramp, a larger one has
+  // fewer launch tails.  Measured on 2.8e9 page-locked nnz (ms per call):
+  // 32M 434-437, 48M 428-432, 64M 429-436, 96M 438-441, and 447-450 for the
+  // earlier blocks that grew by 8% up to 256M.  Pageable inputs go through
+  // pinned staging, which is cheaper to allocate (and re-fill) in blocks of
+  // at most 32M.
   uint64_t block_nnz =
-      pin_in ? std::min<uint64_t>(std::max<uint64_t>(nnz / 8, 8ull << 20), 256ull << 20)
+      pin_in ? std::min<uint64_t>(std::max<uint64_t>(nnz / 8, 8ull << 20), 48ull << 20)
              : std::min<uint64_t>(std::max<uint64_t>(nnz / 16, 4ull << 20), 32ull << 20);
   const int forced = env_int("MHCUDA_B200_BLOCK_NNZ", 0);
   if (forced > 0) block_nnz = static_cast<uint64_t>(forced);
@@ -615,10 +683,7 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
   // Blocks [r0, r1): as many rows as fit the block's nnz (at least one).
   // Hashing cannot start before the first block has crossed the bus, so the
   // first block is small -- 16M nnz, still a few waves of warp items -- and
-  // later ones grow geometrically to block_nnz; the factor keeps each block's
-  // copy-in (8 B per nnz) shorter than the previous block's hashing (samples
-  // evals per nnz), with slack: max(1.08, samples / 120) on a B200 with a
-  // Gen5 x16 link.
+  // later ones double up to block_nnz, where they stay.
   // MHCUDA_B200_BLOCK_NNZ gives constant blocks.
   struct Block {
     uint32_t r0, r1;
@@ -627,8 +692,7 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
   {
     uint64_t cur = forced > 0 ? block_nnz
                               : std::min(block_nnz, std::max<uint64_t>(block_nnz / 32, 16ull << 20));
-    const double growth =
-        forced > 0 ? 1.0 : std::min(2.0, std::max(1.08, gen->samples / 120.0));
+    const double growth = forced > 0 ? 1.0 : 2.0;
     for (uint32_t r0 = 0; r0 < length;) {
       const uint64_t limit = static_cast<uint64_t>(rows[r0]) + cur;
       uint32_t r1 = static_cast<uint32_t>(
@@ -688,6 +752,8 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
   }
 
   MHCUDAResult r = mhcudaSuccess;
+  PipeTrace trace(blocks.size());
+  size_t issued = 0;
   for (uint32_t i = 0; i < blocks.size() && r == mhcudaSuccess; ++i) {
     const uint32_t r0 = blocks[i].r0, r1 = blocks[i].r1;
     Gen::Slot &sl = gen->slots[i % Gen::kPipeSlots];
@@ -722,6 +788,8 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
       src_c = sl.hc.ptr;
       src_i = sl.hip.ptr;
     }
+    trace.nnz(i, n);
+    trace.mark(i, PipeTrace::kH2dStart, gen->s_in);
     MHB_CHECK(gen, cudaMemcpyAsync(sl.ip.ptr, src_i, (static_cast<size_t>(len) + 1) * 4,
                                    cudaMemcpyHostToDevice, gen->s_in),
               mhcudaMemoryCopyError);
@@ -742,8 +810,10 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
                   mhcudaMemoryCopyError);
       }
     }
+    trace.mark(i, PipeTrace::kH2dEnd, gen->s_in);
     MHB_CHECK(gen, cudaEventRecord(sl.h2d, gen->s_in), mhcudaRuntimeError);
     MHB_CHECK(gen, cudaStreamWaitEvent(st, sl.h2d, 0), mhcudaRuntimeError);
+    trace.mark(i, PipeTrace::kHashStart, st);
     const HashPlan plan = make_plan(gen, n, len, force);
     HashArgs a{};
     r = prepare_launch(gen, len, n, plan, &a);
@@ -760,8 +830,10 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
     a.out = sl.out.as<uint32_t>();
     r = enqueue_hash(gen, a, plan, st, /*clear_status=*/false);
     if (r != mhcudaSuccess) break;
+    trace.mark(i, PipeTrace::kHashEnd, st);
     MHB_CHECK(gen, cudaEventRecord(sl.done, st), mhcudaRuntimeError);
     MHB_CHECK(gen, cudaStreamWaitEvent(gen->s_out, sl.done, 0), mhcudaRuntimeError);
+    trace.mark(i, PipeTrace::kD2hStart, gen->s_out);
     uint32_t *dst = output + static_cast<size_t>(r0) * gen->samples * 2;
     if (pin_out) {
       MHB_CHECK(gen, cudaMemcpyAsync(dst, sl.out.ptr, len * row_bytes, cudaMemcpyDeviceToHost,
@@ -775,8 +847,10 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
       sl.pending_out = dst;
       sl.pending_bytes = len * row_bytes;
     }
+    trace.mark(i, PipeTrace::kD2hEnd, gen->s_out);
     MHB_CHECK(gen, cudaEventRecord(sl.d2h, gen->s_out), mhcudaRuntimeError);
     sl.busy = true;
+    issued = i + 1;
     MHB_DEBUG(gen, "block %u: rows [%u, %u) nnz %u chunk %u\n", i, r0, r1, n, plan.chunk);
   }
   for (auto &sl : gen->slots) {
@@ -787,6 +861,7 @@ MHCUDAResult calc_pipelined(const Gen *gen, const HostCsr &in, uint32_t length,
     cudaDeviceSynchronize();
     return r;
   }
+  trace.write(issued);
   return read_status(gen, st);
 }
 
