@@ -134,12 +134,12 @@ struct TuneChoice {
 };
 
 // The autotuner's two choices for a shape class.  `alone` is the fastest
-// candidate of all; `streamed` the fastest with 3 or 4 resident blocks per SM,
-// for launches that run beside host<->device copies (the mhcuda_calc
-// pipeline): the copies share HBM with the kernel's gathers and lengthen their
-// latency, which the 2-block budget, with half the resident warps, hides worst
-// (on a 2,000,000-row Zipf matrix its blocks were 7% slower end to end than
-// 4-block ones, although 3% faster alone).
+// candidate of all; `streamed` the fastest with 4 resident blocks per SM, for
+// the mhcuda_calc pipeline, whose row blocks (up to 48M nnz) run beside
+// host<->device copies.  There the budgets with fewer, longer-running warps
+// lose: on a 2,000,000-row Zipf matrix that the 2-block kernel hashes fastest
+// alone (385 against 415 ms), a pipelined call took 428-430 ms with 4 blocks
+// per SM, 437-440 with 3 and 451-453 with 2.
 struct TunedShape {
   TuneChoice alone, streamed;
 };
@@ -186,8 +186,9 @@ struct MinhashCudaGenerator_ {
   // Grow-only workspace.
   mutable DevBuf d_weights, d_cols, d_indptr, d_out, d_chunk_row, d_part_ln, d_part_kt, d_status;
   mutable PinnedBuf h_status;
-  // Row-block pipeline of mhcuda_calc: two slots, each a block's device CSR,
-  // hashes and (for pageable caller buffers) pinned staging.
+  // Row-block pipelines of mhcuda_calc and mhcuda_calc_batch: three slots,
+  // each a block's device CSR, hashes and (for pageable caller buffers)
+  // pinned staging.
   struct Slot {
     DevBuf w, c, ip, out;
     PinnedBuf hw, hc, hip, hout;
@@ -1533,7 +1534,7 @@ enum MHCUDAResult mhcuda_autotune(const MinhashCudaGenerator *gen, const float *
       best_t = ms / 2;
       best = c;
     }
-    if (c.minb != 2 && ms / 2 < best_streamed_t) {
+    if (c.minb == 4 && ms / 2 < best_streamed_t) {
       best_streamed_t = ms / 2;
       best_streamed = c;
     }
