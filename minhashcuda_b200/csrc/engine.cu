@@ -134,12 +134,12 @@ struct TuneChoice {
 };
 
 // The autotuner's two choices for a shape class.  `alone` is the fastest
-// candidate of all; `streamed` the fastest with 4 resident blocks per SM, for
-// the mhcuda_calc pipeline, whose row blocks (up to 48M nnz) run beside
-// host<->device copies.  There the budgets with fewer, longer-running warps
-// lose: on a 2,000,000-row Zipf matrix that the 2-block kernel hashes fastest
-// alone (385 against 415 ms), a pipelined call took 428-430 ms with 4 blocks
-// per SM, 437-440 with 3 and 451-453 with 2.
+// candidate of all; `streamed` the fastest with the same samples per lane and
+// 4 resident blocks per SM, for the mhcuda_calc pipeline, whose row blocks (up
+// to 48M nnz) run beside host<->device copies.  There the budgets with fewer,
+// longer-running warps lose: on a 2,000,000-row Zipf matrix that the 2-block
+// kernel hashes fastest alone (385 against 415 ms), a pipelined call took
+// 428-430 ms with 4 blocks per SM, 437-440 with 3 and 451-453 with 2.
 struct TunedShape {
   TuneChoice alone, streamed;
 };
@@ -1509,8 +1509,9 @@ enum MHCUDAResult mhcuda_autotune(const MinhashCudaGenerator *gen, const float *
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   MHB_CHECK(gen, cudaEventCreate(&e0), mhcudaRuntimeError);
   MHB_CHECK(gen, cudaEventCreate(&e1), mhcudaRuntimeError);
-  TuneChoice best{}, best_streamed{};
-  double best_t = 1e300, best_streamed_t = 1e300;
+  TuneChoice best{};
+  double best_t = 1e300;
+  std::vector<double> times;
   MHCUDAResult r = mhcudaSuccess;
   for (const TuneChoice &c : cands) {
     const HashPlan plan = make_plan(gen, nnz, length, &c);
@@ -1530,12 +1531,20 @@ enum MHCUDAResult mhcuda_autotune(const MinhashCudaGenerator *gen, const float *
     float ms = 0.0f;
     MHB_CHECK(gen, cudaEventElapsedTime(&ms, e0, e1), mhcudaRuntimeError);
     MHB_DEBUG(gen, "autotune spl=%u minb=%u waves=%u: %.3f ms\n", c.spl, c.minb, c.waves, ms / 2);
+    times.push_back(ms / 2);
     if (ms / 2 < best_t) {
       best_t = ms / 2;
       best = c;
     }
-    if (c.minb == 4 && ms / 2 < best_streamed_t) {
-      best_streamed_t = ms / 2;
+  }
+  // For the pipeline: the winner's samples per lane, 4 blocks per SM, the
+  // fastest chunk granularity among those.
+  TuneChoice best_streamed = best;
+  double best_streamed_t = 1e300;
+  for (size_t i = 0; i < times.size(); ++i) {
+    const TuneChoice &c = cands[i];
+    if (c.spl == best.spl && c.minb == 4 && times[i] < best_streamed_t) {
+      best_streamed_t = times[i];
       best_streamed = c;
     }
   }
