@@ -1594,9 +1594,14 @@ enum MHCUDAResult mhcuda_calc_batch(const MinhashCudaGenerator *gen, uint32_t co
   MHB_CHECK(gen, batch_streams(gen), mhcudaRuntimeError);
   const cudaStream_t st = gen->stream;
   const size_t row_bytes = static_cast<size_t>(gen->samples) * 2 * sizeof(uint32_t);
-  // Groups grow to group_nnz (MHCUDA_B200_BATCH_GROUP_NNZ); with
-  // MHCUDA_B200_BLOCK_NNZ every group is that size.
-  uint64_t group_nnz = 64ull << 20;
+  // Groups of group_nnz (MHCUDA_B200_BATCH_GROUP_NNZ, or MHCUDA_B200_BLOCK_NNZ).
+  // A group's host gather and scatter take about as long as its hashing, and
+  // small groups keep them in the host's caches: measured on the 4096-matrix
+  // batch (3.9e8 nnz, 256 samples), ms per call, constant groups of 8M / 12M /
+  // 16M / 24M / 32M / 48M nnz: 202.5 / 204.4 / 203.4 / 222-231 / 218 / 235,
+  // against 206.5 for groups growing from 2M to 16M and 219-220 for the
+  // earlier groups growing from 8M to 64M (device-resident batch: 195-202).
+  uint64_t group_nnz = 16ull << 20;
   const int cap = env_int("MHCUDA_B200_BATCH_GROUP_NNZ", 0);
   if (cap > 0) group_nnz = static_cast<uint64_t>(cap);
   const int forced = env_int("MHCUDA_B200_BLOCK_NNZ", 0);
@@ -1632,17 +1637,16 @@ enum MHCUDAResult mhcuda_calc_batch(const MinhashCudaGenerator *gen, uint32_t co
     return mhcudaSuccess;
   };
 
-  // Groups [m0, m1) of consecutive matrices, planned up front: the first is
-  // small (hashing waits for its gather and copy-in) and later ones grow to
-  // group_nnz; the last is split off small (its copy-out and scatter are left
-  // once hashing ends).  MHCUDA_B200_BLOCK_NNZ gives constant groups.
+  // Groups [m0, m1) of consecutive matrices, planned up front: up to
+  // group_nnz entries and 2^20 rows each (a matrix larger than that is a
+  // group of its own).
   struct Group {
     uint32_t m0, m1;
     uint64_t nnz, rows;
   };
   std::vector<Group> groups;
   {
-    uint64_t cur = forced > 0 ? group_nnz : std::max<uint64_t>(group_nnz / 8, 1);
+    const uint64_t cur = group_nnz;
     for (uint32_t m0 = 0; m0 < count;) {
       uint32_t m1 = m0;
       uint64_t gn = 0, gr = 0;
@@ -1659,22 +1663,6 @@ enum MHCUDAResult mhcuda_calc_batch(const MinhashCudaGenerator *gen, uint32_t co
       }
       groups.push_back(Group{m0, m1, gn, gr});
       m0 = m1;
-      if (forced <= 0) cur = std::min(group_nnz, std::max(cur + 1, cur * 3 / 2));
-    }
-    const uint64_t tail = std::max<uint64_t>(group_nnz / 8, 1);
-    const Group last = groups.back();
-    if (forced <= 0 && last.nnz > 2 * tail && last.m1 - last.m0 > 1) {
-      uint32_t m = last.m1;
-      uint64_t tn = 0, tr = 0;
-      while (m > last.m0 + 1 && tn + nnz_of[m - 1] <= tail) {
-        tn += nnz_of[m - 1];
-        tr += lengths[m - 1];
-        --m;
-      }
-      if (m < last.m1) {
-        groups.back() = Group{last.m0, m, last.nnz - tn, last.rows - tr};
-        groups.push_back(Group{m, last.m1, tn, tr});
-      }
     }
   }
   // Slots and scratch sized once for the largest group (growing a buffer

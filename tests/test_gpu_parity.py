@@ -324,10 +324,9 @@ def test_near_integer_quotients():
                                             ("MHCUDA_B200_BATCH_GROUP_NNZ", 20000),
                                             ("MHCUDA_B200_BATCH_GROUP_NNZ", 3000)])
 def test_batch_groups_and_empty_matrices(monkeypatch, knob, group_nnz):
-    """mhcuda_calc_batch cut into several pipelined groups -- constant ones
-    (MHCUDA_B200_BLOCK_NNZ) or growing from an eighth of the cap with a small
-    last group (MHCUDA_B200_BATCH_GROUP_NNZ) -- including empty matrices and
-    matrices larger than a group, equals one calc per matrix."""
+    """mhcuda_calc_batch cut into several pipelined groups (group size from
+    either knob), including empty matrices and matrices larger than a group,
+    equals one calc per matrix."""
     import ctypes
     rng = np.random.default_rng(group_nnz)
     dim, samples = 3000, 64
